@@ -1,0 +1,190 @@
+/* svg_b200: B200-native Saddle Vertex Graph (SVG) geodesic engine - C ABI.
+ *
+ * The drop-in boundary for the reference's Mesh / SVG host classes
+ * (Mesh.cuh:33-52, SVG.cuh:18-113).  Plain pointers and sizes only; every call
+ * returns an svg_status, never exits, and leaves a message for
+ * svg_last_error() on failure (the reference prints and exit(-1)s through
+ * HANDLE_ERROR, book.cuh:23-33).  One GPU; handles are not thread-safe, like
+ * the reference classes (SVG::searchType is mutable state, SVG.cu:245).
+ *
+ * Geometry is float64 throughout.  Vertex and half-edge ids are int32.
+ * Half-edge 3f+j of face f runs from faces[3f+j] to faces[3f+(j+1)%3].
+ */
+#ifndef SVG_B200_H
+#define SVG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum svg_status {
+    SVG_OK = 0,
+    SVG_ERR_ARG = 1,      /* bad argument or size */
+    SVG_ERR_IO = 2,       /* file cannot be opened / short read */
+    SVG_ERR_CUDA = 3,     /* CUDA runtime error (message has the CUDA text) */
+    SVG_ERR_NOMEM = 4,    /* device or host allocation failed, or over the HBM budget */
+    SVG_ERR_MESH = 5,     /* mesh unusable (no faces, bad index, too large) */
+    SVG_ERR_STATE = 6     /* call out of order (e.g. graph of another mesh) */
+} svg_status;
+
+typedef struct svg_mesh svg_mesh;    /* host half-edge mesh + its device copy */
+typedef struct svg_graph svg_graph;  /* one built SVG, resident on the device */
+
+/* One SVG edge in the reference's on-disk and host layout, SVG::SVGNode
+ * (SVG.cuh:21-27), 40 bytes: adjacent vertex, geodesic length, and the first
+ * and last key points of the geodesic (half-edge id + position along it). */
+typedef struct svg_node {
+    int32_t adj;
+    int32_t pad_;
+    double dist;
+    uint32_t next_to_src_edge;
+    uint32_t next_to_dst_edge;
+    double next_to_src_x;
+    double next_to_dst_x;
+} svg_node;
+
+/* Last error message of this thread ("" if none). */
+const char* svg_last_error(void);
+
+/* Library version string. */
+const char* svg_version(void);
+
+/* ---------------------------------------------------------------- meshes */
+
+/* Mesh::LoadFromFile (Mesh.cu:24-126): OBJ `v x y z` and `f a b c` lines
+ * (1-based), same half-edge numbering, twin pairing, vertex angle sums and
+ * firstEdge as the reference.  Boundary half-edges get twin -1. */
+svg_status svg_mesh_load_obj(const char* path, svg_mesh** out);
+
+/* The same mesh from arrays: pos[3*nv] (x,y,z), faces[3*nf] (0-based). */
+svg_status svg_mesh_from_arrays(int32_t nv, const double* pos, int32_t nf, const int32_t* faces,
+                                svg_mesh** out);
+
+/* Mesh::copyToGPU (Mesh.cu:128-142): upload the structure-of-arrays device
+ * layout.  Builds call it implicitly; an explicit call times the upload. */
+svg_status svg_mesh_upload(svg_mesh* m);
+
+/* Mesh::clear + Mesh::clearGPU (Mesh.cu:144-158). */
+void svg_mesh_free(svg_mesh* m);
+
+svg_status svg_mesh_counts(const svg_mesh* m, int32_t* nv, int32_t* nf, int32_t* ne);
+
+/* Host copies of the loaded structure (any pointer may be NULL): half-edge
+ * start vertex, twin (-1 on the boundary), length; vertex position, angle sum,
+ * firstEdge (the last half-edge leaving the vertex, -1 if isolated). */
+svg_status svg_mesh_export(const svg_mesh* m, int32_t* he_v0, int32_t* he_twin, double* he_len,
+                           double* pos, double* angle, int32_t* first_edge);
+
+/* ------------------------------------------------------------------ build */
+
+typedef enum svg_build_mode {
+    SVG_BUILD_BATCHED = 0,  /* persistent kernel, device work queue, warp-cooperative emission */
+    SVG_BUILD_PLAIN = 1     /* one source per thread, grid-stride, O(V) emission scan (reference form) */
+} svg_build_mode;
+
+typedef struct svg_build_opts {
+    int32_t K;                /* SVG::SetParameters K (SVG.cu:114): ICH stops after K new vertices */
+    uint32_t split_coef;      /* reference split hash size = K*split_coef (default 10, kernel.cu:422) */
+    uint32_t vert_coef;       /* reference vertex hash size = K*vert_coef (default 2) */
+    int32_t win_queue_cap;    /* window queue capacity, pushes beyond it are dropped (reference 1023) */
+    int32_t pseudo_queue_cap; /* pseudo-source queue capacity (reference 1023) */
+    int32_t mode;             /* svg_build_mode */
+    int32_t threads_per_block;/* 0 = autotuned (batched) / 128 (plain, SVG.cuh:11) */
+    int32_t blocks;           /* 0 = autotuned (batched) / 64 (plain, SVG.cuh:10) */
+    int32_t with_paths;       /* 1 = also produce the path-end fields of svg_node */
+    int32_t heavy_first;      /* batched: order the work queue by an estimated cost */
+    int64_t hbm_budget;       /* bytes of scratch the build may hold (0 = automatic) */
+    int32_t source_begin;     /* build rows for sources [source_begin, source_end) only; */
+    int32_t source_end;       /* 0,0 = all vertices */
+} svg_build_opts;
+
+typedef struct svg_build_stats {
+    double ms_total;          /* device time of the build, CUDA events on the build stream */
+    double ms_ich;            /* window-propagation phase */
+    double ms_emit;           /* edge emission (+ compaction) */
+    int64_t windows;          /* windows propagated */
+    int64_t windows_generated;/* windows created (reference numOfWinGen, summed) */
+    int64_t pseudo_sources;   /* pseudo-sources expanded */
+    int64_t edges;            /* SVG edges emitted */
+    int32_t sources;
+    int32_t max_win_queue;    /* queue high-water marks over all sources */
+    int32_t max_pseudo_queue;
+    int32_t queue_drop_sources; /* sources whose queue was full at a push (reference drops too) */
+    int32_t ref_overflow_sources; /* sources where the reference's fixed hash tables overflow: results
+                                     follow a map without overflow there, not the reference */
+    int32_t watchdog_sources; /* sources stopped by an iteration cap (reference would spin) */
+    int32_t undefined_sources;/* sources reaching a step the reference leaves undefined */
+    int32_t retried_sources;  /* sources re-run with larger scratch tables */
+    int32_t launches;         /* kernels launched */
+    int64_t scratch_bytes;    /* device scratch held by the build */
+} svg_build_stats;
+
+void svg_build_opts_default(svg_build_opts* o);
+
+/* SVG::SetParameters + Allocation + ConstructSVG + Free (SVG.cu:114-182):
+ * build the SVG of mesh m on the device.  The graph stays resident. */
+svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out);
+
+svg_status svg_graph_stats(const svg_graph* g, svg_build_stats* st);
+
+/* Per-source counters (any pointer may be NULL), n = number of built sources:
+ * windows propagated, window-queue high-water mark, flags (bit0 queue drop,
+ * bit1 reference-table overflow, bit2 watchdog, bit3 reference-undefined). */
+svg_status svg_graph_source_stats(const svg_graph* g, int32_t* windows, int32_t* max_queue, int32_t* flags);
+
+/* SVG::FreeSVGStructure (SVG.cu:149-155). */
+void svg_graph_free(svg_graph* g);
+
+/* Vertex count, edge count, K of the build. */
+svg_status svg_graph_counts(const svg_graph* g, int32_t* nv, int64_t* nnz, int32_t* K);
+
+/* SVG::CopySVGToHost (SVG.cu:184-206), as CSR: offsets[nv+1], adj[nnz],
+ * dist[nnz] (any may be NULL).  Rows are in ascending adjacent-vertex order,
+ * row v holding at most K edges, exactly the reference's d_svg rows. */
+svg_status svg_graph_copy_csr(const svg_graph* g, int64_t* offsets, int32_t* adj, double* dist);
+
+/* Full reference-layout rows: tails[nv] and nodes[nnz] (packed CSR order). */
+svg_status svg_graph_copy_nodes(const svg_graph* g, int32_t* tails, svg_node* nodes);
+
+/* Device pointers of the resident CSR (for callers that keep data on the GPU). */
+svg_status svg_graph_device_csr(const svg_graph* g, const int64_t** offsets, const int32_t** adj,
+                                const double** dist);
+
+/* SVG::SaveSVGToFile / LoadSVGFromFile (SVG.cu:208-239): per vertex an int32
+ * degree then degree svg_nodes; no header.  Files are interchangeable with
+ * the reference's. */
+svg_status svg_graph_save(const svg_graph* g, const char* path);
+svg_status svg_graph_load(svg_mesh* m, int32_t K, const char* path, svg_graph** out);
+
+/* ---------------------------------------------------------------- queries */
+
+/* SVG::SolveSSSD (SVG.cu:241-251): shortest SVG distance from s[i] to t[i]
+ * for n pairs in one batch (DBL_MAX if unreachable).  Host buffers. */
+svg_status svg_sssd_batch(svg_graph* g, int32_t n, const int32_t* s, const int32_t* t, double* dist);
+
+/* SVG::SolveMSAD (SVG.cu:354-366): n independent source sets; set q is
+ * srcs[set_offsets[q] .. set_offsets[q+1]) with weights (initial distances).
+ * dist[q*nv + v] receives the distance of v from set q; src_id (optional)
+ * the source whose tree reached v.  A source listed twice keeps the weight
+ * of its last occurrence, as the reference does.  Host buffers. */
+svg_status svg_msad_batch(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs,
+                          const double* weights, double* dist, int32_t* src_id);
+
+/* Same queries on device-resident inputs/outputs (no host copies). */
+svg_status svg_sssd_batch_device(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t,
+                                 double* d_dist);
+svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_offsets,
+                                 const int32_t* d_srcs, const double* d_weights, double* d_dist,
+                                 int32_t* d_src_id);
+
+/* Synchronise the library's stream; returns the device time in ms since the
+ * previous svg_timer_mark (CUDA events on the library stream). */
+svg_status svg_timer_mark(double* ms_since_last);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -26,7 +26,8 @@
 
 #define REF_PI 3.141592653589793238     /* Geometry.cuh:18 */
 #define RELATIVE_ERROR 1e-8             /* ICHDevice.cuh:10 */
-#define WATCHDOG 200000000LL
+#define WATCHDOG (1LL << 26)      /* ICH loop steps per source */
+#define FAN_GUARD (1LL << 20)     /* fan walk / vertex ring steps */
 
 /* ------------------------------------------------------------------ mesh */
 struct om_mesh {
@@ -468,7 +469,7 @@ static void fan_walk(Ich* s, int leftStart, int rightStart, double angle0, doubl
         int op = m->next[cur], nx = m->next[op];
         angle0 += corner(m, cur, nx, op);
         cur = m->twin[nx];
-        if (++guard > WATCHDOG) { s->flags |= 2; return; }
+        if (++guard > FAN_GUARD) { s->flags |= 2; return; }
     }
     if (cur != -1) *startEdge = m->next[m->twin[cur]];
     cur = rightStart;
@@ -476,7 +477,7 @@ static void fan_walk(Ich* s, int leftStart, int rightStart, double angle0, doubl
         int nx = m->next[cur], op = m->next[nx];
         angle1 += corner(m, cur, nx, op);
         cur = m->twin[nx];
-        if (++guard > WATCHDOG) { s->flags |= 2; return; }
+        if (++guard > FAN_GUARD) { s->flags |= 2; return; }
     }
     if (cur != -1) *endEdge = m->twin[m->next[m->next[m->twin[cur]]]];
 }
@@ -533,7 +534,7 @@ static void gen_sub_wins(Ich* s, const PWin* pw) {
         WinQ_push(&s->wq, w, w.minDist);
         ++s->numOfWinGen;
         startEdge = m->twin[m->next[m->next[startEdge]]];
-        if (++guard > WATCHDOG) { s->flags |= 2; break; }
+        if (++guard > FAN_GUARD) { s->flags |= 2; break; }
     } while (startEdge != endEdge);
 
     int start = m->first[pw->vert], cur = start;
@@ -595,9 +596,9 @@ static void trace(Ich* s, int vert, unsigned* nextToSrcEdge, double* nextToSrcX,
     s->pathPassVert = 0;
     *nextToSrcEdge = (unsigned)-1; *nextToDstEdge = (unsigned)-1;
     int curVert = vert;
-    long long guard = 0;
+    long long guard = 0, tcap = 4LL * m->nf + 64;
     while (vget(s, curVert)->dist != 0.0) {
-        if (++guard > WATCHDOG) { s->flags |= 2; return; }
+        if (++guard > tcap) { s->flags |= 2; s->pathPassVert = 1; return; }
         int enterEdge = vget(s, curVert)->enterEdge;
         if (enterEdge == -1) {
             if (*nextToDstEdge == (unsigned)-1) { *nextToDstEdge = m->first[curVert]; *nextToDstX = 0.0; }
@@ -629,7 +630,7 @@ static void trace(Ich* s, int vert, unsigned* nextToSrcEdge, double* nextToSrcX,
             unsigned psrc = (unsigned)sget(s, enterEdge)->psrc;
             if (psrc >= (unsigned)m->nv) { s->flags |= 2; return; }
             while (opv != (int)psrc) {
-                if (++guard > WATCHDOG) { s->flags |= 2; return; }
+                if (++guard > tcap) { s->flags |= 2; s->pathPassVert = 1; return; }
                 int e0 = m->twin[gid], e1 = m->next[e0], e2 = m->next[e1];
                 double L0 = m->len[e0], L1 = m->len[e1], L2 = m->len[e2];
                 vec2 ov;

@@ -1,0 +1,313 @@
+"""svg_b200: B200-native Saddle Vertex Graph geodesics (Python host binding).
+
+A thin ctypes layer over the C ABI of libsvg_b200.so (include/svg_b200.h)
+that mirrors the reference's host classes (Mesh.cuh:33-52, SVG.cuh:18-113):
+
+    mesh = Mesh.LoadFromFile("bunny.obj")        # Mesh::LoadFromFile
+    svg = SVG(); svg.AssignMesh(mesh)             # SVG::AssignMesh
+    svg.SetParameters(100, 10, 2)                 # SVG::SetParameters(K, split, vert)
+    svg.ConstructSVG()                            # SVG::ConstructSVG (on the GPU)
+    offsets, nodes = svg.CopySVGToHost()          # SVG::CopySVGToHost
+    svg.SaveSVGToFile("bunny.svg")                # SVG::SaveSVGToFile (same format)
+    d = svg.SolveSSSD(s, t)                       # SVG::SolveSSSD
+    dist, src = svg.SolveMSAD(srcs, weights)      # SVG::SolveMSAD
+
+All compute runs on the GPU through the native library; there is no CPU
+fallback: if the library cannot be loaded, importing a class that needs it
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Mesh", "SVG", "BuildOptions", "SvgError", "lib", "NODE_DTYPE", "LIB_PATH",
+           "MODE_BATCHED", "MODE_PLAIN"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsvg_b200.so")
+MODE_BATCHED, MODE_PLAIN = 0, 1
+DBL_MAX = np.finfo(np.float64).max
+
+# svg_node: the reference's SVGNode layout (SVG.cuh:21-27), 40 bytes
+NODE_DTYPE = np.dtype([
+    ("adj", np.int32), ("pad", np.int32), ("dist", np.float64),
+    ("src_edge", np.uint32), ("dst_edge", np.uint32),
+    ("src_x", np.float64), ("dst_x", np.float64),
+])
+
+STATUS = {0: "ok", 1: "bad argument", 2: "io", 3: "cuda", 4: "out of memory", 5: "mesh", 6: "state"}
+
+
+class SvgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"svg_b200 error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [
+        ("K", C.c_int32), ("split_coef", C.c_uint32), ("vert_coef", C.c_uint32),
+        ("win_queue_cap", C.c_int32), ("pseudo_queue_cap", C.c_int32), ("mode", C.c_int32),
+        ("threads_per_block", C.c_int32), ("blocks", C.c_int32), ("with_paths", C.c_int32),
+        ("heavy_first", C.c_int32), ("hbm_budget", C.c_int64),
+        ("source_begin", C.c_int32), ("source_end", C.c_int32),
+    ]
+
+
+class BuildStats(C.Structure):
+    _fields_ = [
+        ("ms_total", C.c_double), ("ms_ich", C.c_double), ("ms_emit", C.c_double),
+        ("windows", C.c_int64), ("windows_generated", C.c_int64), ("pseudo_sources", C.c_int64),
+        ("edges", C.c_int64), ("sources", C.c_int32), ("max_win_queue", C.c_int32),
+        ("max_pseudo_queue", C.c_int32), ("queue_drop_sources", C.c_int32),
+        ("ref_overflow_sources", C.c_int32), ("watchdog_sources", C.c_int32),
+        ("undefined_sources", C.c_int32), ("retried_sources", C.c_int32), ("launches", C.c_int32),
+        ("scratch_bytes", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = C.c_void_p
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+# every symbol include/svg_b200.h declares
+EXPORTS = [
+    "svg_last_error", "svg_version", "svg_mesh_load_obj", "svg_mesh_from_arrays", "svg_mesh_upload",
+    "svg_mesh_free", "svg_mesh_counts", "svg_mesh_export", "svg_build_opts_default", "svg_build",
+    "svg_graph_stats", "svg_graph_source_stats", "svg_graph_free", "svg_graph_counts", "svg_graph_copy_csr",
+    "svg_graph_copy_nodes", "svg_graph_device_csr", "svg_graph_save", "svg_graph_load", "svg_sssd_batch",
+    "svg_msad_batch", "svg_sssd_batch_device", "svg_msad_batch_device", "svg_timer_mark",
+]
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libsvg_b200.so (built by svg_b200/build_ext.py).  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"native library missing: {LIB_PATH} (run python -m svg_b200.build_ext)")
+    L = C.CDLL(LIB_PATH)
+    L.svg_last_error.restype = C.c_char_p
+    L.svg_version.restype = C.c_char_p
+    L.svg_mesh_load_obj.argtypes = [C.c_char_p, C.POINTER(_P)]
+    L.svg_mesh_from_arrays.argtypes = [C.c_int32, _f64p, C.c_int32, _i32p, C.POINTER(_P)]
+    L.svg_mesh_upload.argtypes = [_P]
+    L.svg_mesh_free.argtypes = [_P]
+    L.svg_mesh_free.restype = None
+    L.svg_mesh_counts.argtypes = [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.svg_mesh_export.argtypes = [_P] + [_P] * 6
+    L.svg_build_opts_default.argtypes = [C.POINTER(BuildOptions)]
+    L.svg_build_opts_default.restype = None
+    L.svg_build.argtypes = [_P, C.POINTER(BuildOptions), C.POINTER(_P)]
+    L.svg_graph_stats.argtypes = [_P, C.POINTER(BuildStats)]
+    L.svg_graph_source_stats.argtypes = [_P, _P, _P, _P]
+    L.svg_graph_free.argtypes = [_P]
+    L.svg_graph_free.restype = None
+    L.svg_graph_counts.argtypes = [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    L.svg_graph_copy_csr.argtypes = [_P, _P, _P, _P]
+    L.svg_graph_copy_nodes.argtypes = [_P, _P, _P]
+    L.svg_graph_device_csr.argtypes = [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]
+    L.svg_graph_save.argtypes = [_P, C.c_char_p]
+    L.svg_graph_load.argtypes = [_P, C.c_int32, C.c_char_p, C.POINTER(_P)]
+    L.svg_sssd_batch.argtypes = [_P, C.c_int32, _i32p, _i32p, _f64p]
+    L.svg_msad_batch.argtypes = [_P, C.c_int32, _i64p, _P, _P, _f64p, _P]
+    L.svg_sssd_batch_device.argtypes = [_P, C.c_int32, _P, _P, _P]
+    L.svg_msad_batch_device.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P]
+    L.svg_timer_mark.argtypes = [C.POINTER(C.c_double)]
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise SvgError(rc, lib().svg_last_error().decode(errors="replace"))
+
+
+class Mesh:
+    """Half-edge triangle mesh (reference Mesh, Mesh.cuh:33-52)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        nv, nf, ne = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().svg_mesh_counts(handle, C.byref(nv), C.byref(nf), C.byref(ne)))
+        self.vertNum, self.faceNum, self.edgeNum = nv.value, nf.value, ne.value
+
+    @classmethod
+    def LoadFromFile(cls, path: str) -> "Mesh":
+        h = _P()
+        _check(lib().svg_mesh_load_obj(os.fsencode(path), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, pos, faces) -> "Mesh":
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        faces = np.ascontiguousarray(faces, np.int32).reshape(-1)
+        h = _P()
+        _check(lib().svg_mesh_from_arrays(len(pos) // 3, pos, len(faces) // 3, faces, C.byref(h)))
+        return cls(h)
+
+    def copyToGPU(self) -> None:
+        _check(lib().svg_mesh_upload(self._h))
+
+    def clear(self) -> None:
+        if self._h:
+            lib().svg_mesh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+    def export(self) -> dict:
+        V, E = self.vertNum, self.edgeNum
+        out = dict(he_v0=np.zeros(E, np.int32), he_twin=np.zeros(E, np.int32), he_len=np.zeros(E),
+                   pos=np.zeros((V, 3)), angle=np.zeros(V), first_edge=np.zeros(V, np.int32))
+        _check(lib().svg_mesh_export(self._h, *[out[k].ctypes.data_as(_P) for k in
+                                                ["he_v0", "he_twin", "he_len", "pos", "angle", "first_edge"]]))
+        return out
+
+
+class SVG:
+    """Saddle Vertex Graph on the device (reference SVG, SVG.cuh:18-113)."""
+
+    def __init__(self):
+        self.mesh: Mesh | None = None
+        self.K = 100
+        self.splitInfoCoef = 10
+        self.vertInfoCoef = 2
+        self._g = None
+        self.options = BuildOptions()
+        lib().svg_build_opts_default(C.byref(self.options))
+
+    # ---- reference method names
+    def AssignMesh(self, mesh: Mesh, d_mesh=None) -> None:
+        self.mesh = mesh
+
+    def SetParameters(self, K: int, splitInfoCoef: int = 10, vertInfoCoef: int = 2) -> None:
+        self.K, self.splitInfoCoef, self.vertInfoCoef = int(K), int(splitInfoCoef), int(vertInfoCoef)
+
+    def Allocation(self) -> bool:
+        """Scratch is allocated inside ConstructSVG; kept for API parity."""
+        return True
+
+    def Free(self) -> None:
+        """Build scratch is released by the library; kept for API parity."""
+
+    def ConstructSVG(self, mode: int = MODE_BATCHED, with_paths: bool = True, **kw) -> dict:
+        if self.mesh is None:
+            raise SvgError(6, "AssignMesh first")
+        self.FreeSVGStructure()
+        o = BuildOptions()
+        lib().svg_build_opts_default(C.byref(o))
+        o.K, o.split_coef, o.vert_coef = self.K, self.splitInfoCoef, self.vertInfoCoef
+        o.mode = mode
+        o.with_paths = int(with_paths)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        self.options = o
+        h = _P()
+        _check(lib().svg_build(self.mesh._h, C.byref(o), C.byref(h)))
+        self._g = h
+        return self.stats()
+
+    def FreeSVGStructure(self) -> None:
+        if self._g:
+            lib().svg_graph_free(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.FreeSVGStructure()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        st = BuildStats()
+        _check(lib().svg_graph_stats(self._g, C.byref(st)))
+        return st.as_dict()
+
+    def source_stats(self):
+        V = self.mesh.vertNum
+        w, q, f = np.zeros(V, np.int32), np.zeros(V, np.int32), np.zeros(V, np.int32)
+        _check(lib().svg_graph_source_stats(self._g, w.ctypes.data_as(_P), q.ctypes.data_as(_P),
+                                            f.ctypes.data_as(_P)))
+        return w, q, f
+
+    def counts(self):
+        nv, nnz, K = C.c_int32(), C.c_int64(), C.c_int32()
+        _check(lib().svg_graph_counts(self._g, C.byref(nv), C.byref(nnz), C.byref(K)))
+        return nv.value, nnz.value, K.value
+
+    def csr(self):
+        """(offsets[V+1] int64, adj[nnz] int32, dist[nnz] float64) on the host."""
+        nv, nnz, _ = self.counts()
+        off = np.zeros(nv + 1, np.int64)
+        adj = np.zeros(max(nnz, 1), np.int32)
+        dist = np.zeros(max(nnz, 1))
+        _check(lib().svg_graph_copy_csr(self._g, off.ctypes.data_as(_P), adj.ctypes.data_as(_P),
+                                        dist.ctypes.data_as(_P)))
+        return off, adj[:nnz], dist[:nnz]
+
+    def CopySVGToHost(self):
+        """(offsets, nodes): reference-layout rows packed in CSR order."""
+        nv, nnz, _ = self.counts()
+        tails = np.zeros(nv, np.int32)
+        nodes = np.zeros(max(nnz, 1), NODE_DTYPE)
+        _check(lib().svg_graph_copy_nodes(self._g, tails.ctypes.data_as(_P), nodes.ctypes.data_as(_P)))
+        off = np.zeros(nv + 1, np.int64)
+        np.cumsum(tails, out=off[1:])
+        return off, nodes[:nnz]
+
+    def SaveSVGToFile(self, path: str) -> None:
+        _check(lib().svg_graph_save(self._g, os.fsencode(path)))
+
+    def LoadSVGFromFile(self, path: str) -> None:
+        self.FreeSVGStructure()
+        h = _P()
+        _check(lib().svg_graph_load(self.mesh._h, self.K, os.fsencode(path), C.byref(h)))
+        self._g = h
+
+    # ---- queries
+    def sssd_batch(self, s, t) -> np.ndarray:
+        s = np.ascontiguousarray(s, np.int32)
+        t = np.ascontiguousarray(t, np.int32)
+        d = np.zeros(len(s))
+        _check(lib().svg_sssd_batch(self._g, len(s), s, t, d))
+        return d
+
+    def SolveSSSD(self, s: int, t: int) -> float:
+        return float(self.sssd_batch([s], [t])[0])
+
+    def msad_batch(self, sets, weights=None, with_src: bool = True):
+        """sets: list of source-id arrays; weights: list of weight arrays (default 0)."""
+        V = self.mesh.vertNum
+        n = len(sets)
+        off = np.zeros(n + 1, np.int64)
+        np.cumsum([len(x) for x in sets], out=off[1:])
+        srcs = np.ascontiguousarray(np.concatenate(sets) if n else np.zeros(0), np.int32)
+        if weights is None:
+            w = np.zeros(len(srcs))
+        else:
+            w = np.ascontiguousarray(np.concatenate(weights) if n else np.zeros(0), np.float64)
+        dist = np.zeros(n * V)
+        sid = np.zeros(n * V, np.int32) if with_src else None
+        _check(lib().svg_msad_batch(self._g, n, off, srcs.ctypes.data_as(_P), w.ctypes.data_as(_P), dist,
+                                    sid.ctypes.data_as(_P) if with_src else None))
+        dist = dist.reshape(n, V)
+        return (dist, sid.reshape(n, V)) if with_src else dist
+
+    def SolveMSAD(self, sources, sourceWeights):
+        d, s = self.msad_batch([np.asarray(sources)], [np.asarray(sourceWeights, np.float64)])
+        return d[0], s[0]

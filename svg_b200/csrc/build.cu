@@ -1,0 +1,759 @@
+// SVG construction kernels and their host orchestration.
+//
+//  batched (the product path):
+//    k_ich_batched  persistent: every lane pulls sources from a device work
+//                   queue, runs one K-limited ICH, classifies the vertices it
+//                   reached (direct = geodesic passes no vertex, decided from
+//                   the first back-trace hop) and appends the direct ones to a
+//                   candidate pool.  The loop is flat - one ICH step per
+//                   iteration - so a lane that finishes takes new work at once
+//                   instead of idling until its warp's slowest source ends.
+//    exclusive scan of the per-source degrees -> CSR offsets
+//    k_emit         one warp per source: bitonic-sort the candidates by vertex
+//                   id in shared memory, keep the first K (the reference's
+//                   ascending-j, cap-K rule, SVG.cu:44-75), trace their path
+//                   ends in parallel, write the CSR row.
+//  plain (the reference's form, for comparison):
+//    k_ich_plain    one source per thread, grid-stride, full table reset per
+//                   source and the O(V) emission scan of SVG.cu:44-75 with the
+//                   full back-trace, into a V x K padded array; then
+//                   k_compact packs it into the same CSR.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "engine.h"
+#include "ich.cuh"
+
+namespace svgb {
+
+struct PhaseOut {
+    const int32_t* order;
+    int32_t nsrc;
+    int32_t* work;                 // work-queue head
+    int32_t* retry;                // sources whose lane tables filled
+    int32_t* retry_n;
+    Cand* cand;
+    unsigned long long* cand_used;
+    int64_t cand_cap;
+    int64_t* cand_start;           // per vertex
+    int32_t* cand_n;
+    int32_t* deg;
+    int32_t* st_windows;
+    int32_t* st_maxq;
+    int32_t* st_flags;
+    unsigned long long* acc;       // windows, generated, pseudo-sources, queue-drop sources
+};
+
+__device__ void record_stats(const Lane& L, const PhaseOut& O, int v) {
+    O.st_windows[v] = L.windows;
+    O.st_maxq[v] = L.maxw;
+    int f = 0;
+    if (L.flags & kFlagQueueDrop) f |= 1;
+    if (L.flags & kFlagRefOverflow) f |= 2;
+    if (L.flags & kFlagWatchdog) f |= 4;
+    if (L.flags & kFlagUndefined) f |= 8;
+    O.st_flags[v] = f;
+    atomicAdd(&O.acc[0], (unsigned long long)L.windows);
+    atomicAdd(&O.acc[1], (unsigned long long)L.generated);
+    atomicAdd(&O.acc[2], (unsigned long long)L.pseudos);
+    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[3]), (unsigned long long)L.maxw);
+    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[4]), (unsigned long long)L.maxp);
+}
+
+// End of one source in the batched kernel: export the direct candidates.
+// BuildGeodesicPathTo (ICHDevice.cu:336-480) sets pathPassVert on its first
+// hop already: through a vertex that is not the source (enterEdge starts at
+// the vertex, or a window chain whose pseudo-source is another vertex), or
+// through enterEdge -1.  A vertex at distance 0 has no key point at all.
+__device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
+    const DevMesh& M = L.C.M;
+    if (L.flags & kFlagCapacity) {
+        int k = atomicAdd(O.retry_n, 1);
+        O.retry[k] = v;
+        return;
+    }
+    unsigned long long base = atomicAdd(O.cand_used, (unsigned long long)L.vcount);
+    record_stats(L, O, v);
+    if (base + (unsigned long long)L.vcount > (unsigned long long)O.cand_cap) {
+        O.cand_n[v] = 0;
+        O.deg[v] = 0;
+        return;  // the host sees cand_used > cand_cap and reruns with a larger pool
+    }
+    int n = 0;
+    for (int i = 0; i < L.vcount; ++i) {
+        int u = L.VL[i];
+        int s = L.vfind(u);
+        double d = L.VT[s].dist;
+        if (d == DBL_MAX || u == v) continue;
+        Cand c;
+        c.u = u;
+        c.dist = d;
+        c.ee = -1;
+        c.x = 0.0;
+        bool direct;
+        if (d == 0.0) {
+            direct = true;
+        } else {
+            int enter = L.VT[s].enter;
+            if (enter == -1) {
+                direct = false;
+            } else {
+                HeRec h = ld_he(M.he, enter);
+                if (h.v0 == u) {
+                    direct = (h.v1 == v);
+                } else {
+                    int ss = L.sfind(enter);
+                    int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
+                    if ((unsigned)psrc >= (unsigned)M.nv) {
+                        L.flags |= kFlagUndefined;
+                        direct = false;
+                    } else {
+                        direct = (psrc == v);
+                        c.ee = enter;
+                        c.x = L.ST[ss].x;
+                    }
+                }
+            }
+        }
+        if (direct) O.cand[base + n++] = c;
+    }
+    O.cand_start[v] = (int64_t)base;
+    O.cand_n[v] = n;
+    O.deg[v] = min(n, L.C.K);
+    if (L.flags & kFlagUndefined) O.st_flags[v] |= 8;
+}
+
+__global__ void __launch_bounds__(128) k_ich_batched(LaneConfig C, PhaseOut O) {
+    int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    Lane L(C, gtid);
+    int r = atomicAdd(O.work, 1);
+    int v = r < O.nsrc ? O.order[r] : -1;
+    if (v >= 0) L.begin(v, false);
+    while (v >= 0) {
+        if (L.step()) {
+            finish_batched(L, O, v);
+            r = atomicAdd(O.work, 1);
+            v = r < O.nsrc ? O.order[r] : -1;
+            if (v >= 0) L.begin(v, false);
+        }
+    }
+    L.save_epoch(gtid);
+}
+
+// BuildGeodesicPathTo(vertex) (ICHDevice.cu:336-480), the full back-trace the
+// plain emission runs for every reached vertex.  Returns pathPassVert.
+__device__ bool trace_full(Lane& L, int vert, uint32_t& se, double& sx, uint32_t& de, double& dx) {
+    const DevMesh& M = L.C.M;
+    bool pass = false;
+    se = 0xFFFFFFFFu;
+    de = 0xFFFFFFFFu;
+    int curVert = vert;
+    int guard = 0;
+    for (;;) {
+        int s = L.vfind(curVert);
+        double d = s < 0 ? DBL_MAX : L.VT[s].dist;
+        if (d == 0.0) break;
+        if (++guard > M.nf + 8) { L.flags |= kFlagWatchdog; return true; }
+        int enterEdge = s < 0 ? -1 : L.VT[s].enter;
+        if (enterEdge == -1) {
+            if (de == 0xFFFFFFFFu) { de = (uint32_t)__ldg(&M.vr[curVert].first); dx = 0.0; }
+            else { se = (uint32_t)__ldg(&M.vr[curVert].first); sx = 0.0; }
+            return true;
+        }
+        HeRec he = ld_he(M.he, enterEdge);
+        if (he.v0 == curVert) {
+            int nextVert = he.v1;
+            if (nextVert != L.source) {
+                if (de == 0xFFFFFFFFu) { de = (uint32_t)nxt(enterEdge); dx = 0.0; }
+                else { se = (uint32_t)nxt(enterEdge); sx = 0.0; }
+                pass = true;
+            }
+            curVert = nextVert;
+            continue;
+        }
+        int ss = L.sfind(enterEdge);
+        double gpos = ss < 0 ? DBL_MAX : L.ST[ss].x;
+        int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
+        int gid = enterEdge;
+        if (de == 0xFFFFFFFFu) { de = (uint32_t)gid; dx = gpos; }
+        else { se = (uint32_t)gid; sx = gpos; }
+        if ((unsigned)psrc >= (unsigned)M.nv || he.twin < 0) { L.flags |= kFlagUndefined; return true; }
+        int opv = ld_he(M.he, nxt(he.twin)).v1;
+        double2 last = ld_apex(M.geo, gid);
+        double cx = he.len - gpos, cy = 0.0;
+        HeRec hg = he;
+        while (opv != psrc) {
+            if (++guard > M.nf + 8) { L.flags |= kFlagWatchdog; return true; }
+            int e0 = hg.twin, e1 = nxt(e0), e2 = nxt(e1);
+            double L0 = ld_he(M.he, e0).len, L1 = ld_he(M.he, e1).len, L2 = ld_he(M.he, e2).len;
+            double2 ov = ld_top(M.geo, e0);
+            double s_ = gpos / L0, t_ = 1.0 - gpos / L0;
+            double2 nl;
+            if (to_left(ov.x, ov.y, last.x, last.y, cx, cy)) {
+                double2 p0 = ld_apex(M.geo, e1);
+                nl.x = p0.x * s_ + L1 * t_;
+                nl.y = p0.y * s_ + 0.0 * t_;
+                gpos = isect(last.x, last.y, cx, cy, L0, 0.0, ov.x, ov.y);
+                gpos = (1.0 - gpos) * L1;
+                gid = e1;
+                cx = L1 - gpos;
+            } else {
+                double2 p1 = ld_apex(M.geo, e2);
+                nl.x = 0.0 * s_ + p1.x * t_;
+                nl.y = 0.0 * s_ + p1.y * t_;
+                gpos = isect(last.x, last.y, cx, cy, ov.x, ov.y, 0.0, 0.0);
+                gpos = (1.0 - gpos) * L2;
+                gid = e2;
+                cx = L2 - gpos;
+            }
+            cy = 0.0;
+            last = nl;
+            se = (uint32_t)gid;
+            sx = gpos;
+            hg = ld_he(M.he, gid);
+            if (hg.twin < 0) { L.flags |= kFlagUndefined; return true; }
+            opv = ld_he(M.he, nxt(hg.twin)).v1;
+        }
+        if (opv != L.source) {
+            se = (uint32_t)__ldg(&M.vr[opv].first);
+            sx = 0.0;
+            pass = true;
+        }
+        curVert = opv;
+    }
+    return pass;
+}
+
+struct PlainOut {
+    const int32_t* order;
+    int32_t nsrc;
+    int32_t* tails;        // per row
+    int32_t* adj;          // nsrc*K padded rows
+    double* dist;
+    PathEnd* path;
+    PhaseOut stats;
+};
+
+// constructSVG (SVG.cu:9-96): one source per thread, grid-stride.
+__global__ void __launch_bounds__(128) k_ich_plain(LaneConfig C, PlainOut O) {
+    int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    int stride = gridDim.x * blockDim.x;
+    Lane L(C, gtid);
+    const int K = C.K;
+    for (int r = gtid; r < O.nsrc; r += stride) {
+        int v = O.order[r];
+        L.begin(v, true);
+        while (!L.step()) {
+        }
+        int tail = 0;
+        size_t row = (size_t)r * K;
+        if (!(L.flags & kFlagCapacity)) {
+            for (int j = 0; j < C.M.nv && K > 0; ++j) {
+                double d = L.vdist(j);
+                if (d == DBL_MAX || j == v) continue;
+                uint32_t se, de;
+                double sx = 0.0, dx = 0.0;
+                if (trace_full(L, j, se, sx, de, dx)) continue;
+                if (se == 0xFFFFFFFFu) { se = de; sx = dx; }
+                O.adj[row + tail] = j;
+                O.dist[row + tail] = d;
+                if (O.path) {
+                    PathEnd pe;
+                    pe.src_edge = se; pe.dst_edge = de; pe.src_x = sx; pe.dst_x = dx;
+                    O.path[row + tail] = pe;
+                }
+                if (++tail == K) break;
+            }
+        }
+        O.tails[r] = tail;
+        O.stats.deg[v] = tail;
+        if (L.flags & kFlagCapacity) {
+            int k = atomicAdd(O.stats.retry_n, 1);
+            O.stats.retry[k] = v;
+        } else {
+            record_stats(L, O.stats, v);
+        }
+    }
+}
+
+struct EmitParams {
+    DevMesh M;
+    int32_t K;
+    int32_t nv;
+    const int32_t* order;
+    int32_t nsrc;
+    const Cand* cand;
+    const int64_t* cand_start;
+    const int32_t* cand_n;
+    const int64_t* off;
+    int32_t* adj;
+    double* dist;
+    PathEnd* path;
+    int32_t* st_flags;
+    int32_t smax;            // sort capacity per warp (power of two)
+};
+
+// Warp-per-source emission.
+__global__ void __launch_bounds__(256) k_emit(EmitParams P) {
+    extern __shared__ unsigned long long sm_keys[];
+    int lane = threadIdx.x & 31;
+    int wib = threadIdx.x >> 5;
+    unsigned long long* keys = sm_keys + (size_t)wib * P.smax;
+    int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = gw; r < P.nsrc; r += nw) {
+        int v = P.order[r];
+        int n = P.cand_n[v];
+        if (n <= 0) continue;
+        int64_t start = P.cand_start[v];
+        int N = 32;
+        while (N < n) N <<= 1;
+        if (N > P.smax) {  // cannot happen: smax covers the largest vertex list
+            if (lane == 0) P.st_flags[v] |= 8;
+            continue;
+        }
+        for (int i = lane; i < N; i += 32)
+            keys[i] = i < n ? ((unsigned long long)(uint32_t)P.cand[start + i].u << 32) | (uint32_t)i
+                            : ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= N; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < N; i += 32) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        unsigned long long a = keys[i], b = keys[ixj];
+                        bool up = (i & k) == 0;
+                        if ((a > b) == up) {
+                            keys[i] = b;
+                            keys[ixj] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        int deg = min(n, P.K);
+        int64_t base = P.off[v];
+        int fl = 0;
+        for (int i = lane; i < deg; i += 32) {
+            int idx = (int)(keys[i] & 0xFFFFFFFFu);
+            Cand c = P.cand[start + idx];
+            P.adj[base + i] = c.u;
+            P.dist[base + i] = c.dist;
+            if (P.path) {
+                PathEnd pe;
+                if (c.ee < 0) {
+                    pe.src_edge = pe.dst_edge = 0xFFFFFFFFu;
+                    pe.src_x = pe.dst_x = 0.0;
+                } else {
+                    pe.dst_edge = (uint32_t)c.ee;
+                    pe.dst_x = c.x;
+                    trace_direct(P.M, v, c.ee, c.x, pe.src_edge, pe.src_x, fl);
+                    if (pe.src_edge == 0xFFFFFFFFu) {
+                        pe.src_edge = pe.dst_edge;
+                        pe.src_x = pe.dst_x;
+                    }
+                }
+                P.path[base + i] = pe;
+            }
+        }
+        if (fl) atomicOr(&P.st_flags[v], (fl & kFlagWatchdog) ? 4 : 8);
+        __syncwarp();
+    }
+}
+
+// Pack padded rows (plain build) into CSR.
+__global__ void k_compact(const int32_t* order, int32_t nsrc, int32_t K, const int32_t* tails,
+                          const int32_t* padj, const double* pdist, const PathEnd* ppath, const int64_t* off,
+                          int32_t* adj, double* dist, PathEnd* path) {
+    int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = gw; r < nsrc; r += nw) {
+        int v = order[r];
+        int t = tails[r];
+        int64_t b = off[v];
+        size_t row = (size_t)r * K;
+        for (int i = lane; i < t; i += 32) {
+            adj[b + i] = padj[row + i];
+            dist[b + i] = pdist[row + i];
+            if (path) path[b + i] = ppath[row + i];
+        }
+    }
+}
+
+__global__ void k_iota(int32_t* o, int32_t n, int32_t base) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = base + i;
+}
+
+// ------------------------------------------------------------------ host
+
+namespace {
+
+struct Layout {
+    int32_t lanes = 0, wcap = 0, pcap = 0, vcap_log2 = 0, scap_log2 = 0, vlimit = 0;
+    bool operator==(const Layout& o) const {
+        return lanes == o.lanes && wcap == o.wcap && pcap == o.pcap && vcap_log2 == o.vcap_log2 &&
+               scap_log2 == o.scap_log2 && vlimit == o.vlimit;
+    }
+};
+
+size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+size_t lane_bytes(const Layout& l) {
+    size_t b = 0;
+    b += (size_t)(l.wcap + 1) * sizeof(WinEntry);
+    b += (size_t)l.wcap * sizeof(WinPay);
+    b += (size_t)l.wcap * sizeof(uint16_t);
+    b += (size_t)(l.pcap + 1) * sizeof(PsEntry);
+    b += ((size_t)1 << l.vcap_log2) * sizeof(VSlot);
+    b += (size_t)l.vlimit * sizeof(int32_t);
+    b += ((size_t)1 << l.scap_log2) * sizeof(SSlot);
+    b += sizeof(uint32_t);
+    return b;
+}
+
+// Lane scratch, kept across builds; zeroed when its layout changes so epoch
+// stamps never alias.
+struct Arena {
+    DevBuf buf;
+    Layout layout;
+};
+Arena g_arena[2];  // [0] main pass, [1] retry pass with larger tables
+
+void carve(Arena& A, const Layout& l, LaneConfig& C, cudaStream_t st) {
+    size_t lanes = (size_t)l.lanes;
+    size_t sz[7] = {
+        align_up(lanes * (l.wcap + 1) * sizeof(WinEntry)),
+        align_up(lanes * l.wcap * sizeof(WinPay)),
+        align_up(lanes * l.wcap * sizeof(uint16_t)),
+        align_up(lanes * (l.pcap + 1) * sizeof(PsEntry)),
+        align_up(lanes * ((size_t)1 << l.vcap_log2) * sizeof(VSlot)),
+        align_up(lanes * l.vlimit * sizeof(int32_t)),
+        align_up(lanes * ((size_t)1 << l.scap_log2) * sizeof(SSlot)),
+    };
+    size_t ep = align_up(lanes * sizeof(uint32_t));
+    size_t total = ep;
+    for (size_t s : sz) total += s;
+    bool fresh = !(A.layout == l) || A.buf.bytes < total;
+    if (A.buf.bytes < total) A.buf.reserve(total);
+    char* p = A.buf.as<char>();
+    C.wheap = reinterpret_cast<WinEntry*>(p); p += sz[0];
+    C.wpool = reinterpret_cast<WinPay*>(p); p += sz[1];
+    C.wfree = reinterpret_cast<uint16_t*>(p); p += sz[2];
+    C.pheap = reinterpret_cast<PsEntry*>(p); p += sz[3];
+    C.vtab = reinterpret_cast<VSlot*>(p); p += sz[4];
+    C.vlist = reinterpret_cast<int32_t*>(p); p += sz[5];
+    C.stab = reinterpret_cast<SSlot*>(p); p += sz[6];
+    C.epochs = reinterpret_cast<uint32_t*>(p);
+    if (fresh) {
+        SVG_CUDA(cudaMemsetAsync(C.vtab, 0, sz[4], st));
+        SVG_CUDA(cudaMemsetAsync(C.stab, 0, sz[6], st));
+        SVG_CUDA(cudaMemsetAsync(C.epochs, 0, ep, st));
+        A.layout = l;
+    }
+}
+
+int ilog2_ceil(int64_t x) {
+    int k = 0;
+    while (((int64_t)1 << k) < x) ++k;
+    return k;
+}
+
+}  // namespace
+
+svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
+    upload_mesh(m);
+    cudaStream_t st = lib_stream();
+    const HostMesh& H = m->h;
+    const int32_t nv = H.nv;
+    const int32_t K = o.K;
+    int32_t sb = o.source_begin, se = o.source_end;
+    if (sb == 0 && se == 0) se = nv;
+    if (sb < 0 || se > nv || sb > se) throw SvgError{SVG_ERR_ARG, "source range outside [0, nv]"};
+    if (K <= 0 && K != -1) throw SvgError{SVG_ERR_ARG, "K must be positive"};
+    if (K == -1) throw SvgError{SVG_ERR_ARG, "exhaustive ICH (K=-1) is not a build mode"};
+    if (o.win_queue_cap < 1 || o.win_queue_cap > 65535 || o.pseudo_queue_cap < 1)
+        throw SvgError{SVG_ERR_ARG, "queue capacities must be in [1, 65535]"};
+    const int32_t nsrc = se - sb;
+    const bool plain = o.mode == SVG_BUILD_PLAIN;
+
+    int dev = 0;
+    SVG_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    SVG_CUDA(cudaGetDeviceProperties(&prop, dev));
+
+    LaneConfig C{};
+    C.M = m->d.view();
+    C.K = K;
+    C.wcap = o.win_queue_cap;
+    C.pcap = o.pseudo_queue_cap;
+    C.vref = (uint32_t)K * o.vert_coef;
+    C.sref = (uint32_t)K * o.split_coef;
+    C.watchdog = (int64_t)1 << 26;
+    Layout lay;
+    lay.wcap = C.wcap;
+    lay.pcap = C.pcap;
+    lay.vcap_log2 = std::max(6, ilog2_ceil(2 * ((int64_t)C.vref + 1)));
+    lay.scap_log2 = std::max(8, ilog2_ceil(4 * (int64_t)K));
+    lay.vlimit = (int32_t)(((int64_t)3 << lay.vcap_log2) / 4);
+    C.vcap_log2 = lay.vcap_log2;
+    C.scap_log2 = lay.scap_log2;
+    C.vlimit = lay.vlimit;
+    C.slimit = (int32_t)(((int64_t)3 << lay.scap_log2) / 4);
+
+    size_t freeb = 0, totalb = 0;
+    SVG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+    int64_t budget = o.hbm_budget > 0 ? o.hbm_budget : (int64_t)((double)freeb * 0.5);
+
+    int tpb = o.threads_per_block > 0 ? o.threads_per_block : 128;
+    if (tpb % 32 != 0 || tpb > 128) throw SvgError{SVG_ERR_ARG, "threads_per_block must be a multiple of 32, <= 128"};
+    int blocks = o.blocks;
+    if (plain) {
+        if (blocks <= 0) blocks = 64;  // SVG_BLOCK_NUM (SVG.cuh:10)
+        if (o.threads_per_block <= 0) tpb = 128;  // SVG_THREAD_NUM
+    } else if (blocks <= 0) {
+        int per_sm = 0;
+        SVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ich_batched, tpb, 0));
+        blocks = std::max(1, per_sm) * prop.multiProcessorCount;
+    }
+    int64_t want_blocks = (nsrc + tpb - 1) / tpb;
+    if (!plain) blocks = (int)std::min<int64_t>(blocks, std::max<int64_t>(1, want_blocks));
+    lay.lanes = blocks * tpb;
+    while (lay.lanes > 32 && (int64_t)(lane_bytes(lay) * lay.lanes) > budget) {
+        blocks = std::max(1, blocks / 2);
+        lay.lanes = blocks * tpb;
+    }
+    if ((int64_t)(lane_bytes(lay) * lay.lanes) > budget)
+        throw SvgError{SVG_ERR_NOMEM, "HBM budget too small for one block of build lanes"};
+
+    carve(g_arena[0], lay, C, st);
+
+    // per-build buffers
+    DevBuf b_order, b_misc, b_cand, b_candstart;
+    b_order.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1));
+    int32_t* d_order = b_order.as<int32_t>();
+    if (nsrc > 0) k_iota<<<(nsrc + 255) / 256, 256, 0, st>>>(d_order, nsrc, sb);
+    // misc: work, retry_n, acc[8], cand_used ; retry list ; cand_n ; deg
+    // retry list: room for the first pass's failures and, after them, the retry pass's
+    size_t retry_bytes = align_up(sizeof(int32_t) * 2 * (size_t)std::max(nsrc, 1));
+    size_t misc_bytes = 256 + retry_bytes + 2 * align_up(sizeof(int32_t) * ((size_t)nv + 1));
+    b_misc.reserve(misc_bytes);
+    SVG_CUDA(cudaMemsetAsync(b_misc.p, 0, misc_bytes, st));
+    char* mp = b_misc.as<char>();
+    int32_t* d_work = reinterpret_cast<int32_t*>(mp);
+    int32_t* d_retry_n = d_work + 1;
+    unsigned long long* d_acc = reinterpret_cast<unsigned long long*>(mp + 64);
+    unsigned long long* d_cand_used = d_acc + 8;
+    int32_t* d_retry = reinterpret_cast<int32_t*>(mp + 256);
+    int32_t* d_cand_n = reinterpret_cast<int32_t*>(mp + 256 + retry_bytes);
+    int32_t* d_deg = d_cand_n + align_up(sizeof(int32_t) * ((size_t)nv + 1)) / sizeof(int32_t);
+
+    g->nv = nv;
+    g->K = K;
+    g->with_paths = o.with_paths != 0;
+    SVG_CUDA(cudaMalloc(&g->st_windows, sizeof(int32_t) * (size_t)nv * 3));
+    g->st_maxq = g->st_windows + nv;
+    g->st_flags = g->st_maxq + nv;
+    SVG_CUDA(cudaMemsetAsync(g->st_windows, 0, sizeof(int32_t) * (size_t)nv * 3, st));
+    SVG_CUDA(cudaMalloc(&g->off, sizeof(int64_t) * ((size_t)nv + 1)));
+
+    PhaseOut O{};
+    O.order = d_order;
+    O.nsrc = nsrc;
+    O.work = d_work;
+    O.retry = d_retry;
+    O.retry_n = d_retry_n;
+    O.cand_used = d_cand_used;
+    O.cand_n = d_cand_n;
+    O.deg = d_deg;
+    O.st_windows = g->st_windows;
+    O.st_maxq = g->st_maxq;
+    O.st_flags = g->st_flags;
+    O.acc = d_acc;
+
+    cudaEvent_t ev[4];
+    for (auto& e : ev) SVG_CUDA(cudaEventCreate(&e));
+    int launches = 1;  // iota
+    SVG_CUDA(cudaEventRecord(ev[0], st));
+
+    DevBuf b_padj, b_pdist, b_ppath, b_tails;
+    int32_t retry_n = 0;
+    int32_t retry_host_cap_log2_v = lay.vcap_log2 + 1, retry_host_cap_log2_s = lay.scap_log2 + 2;
+    int32_t smax_vlimit = lay.vlimit;
+    int64_t scratch_bytes = (int64_t)(lane_bytes(lay) * lay.lanes);
+
+    if (plain) {
+        b_tails.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1));
+        b_padj.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1) * K);
+        b_pdist.reserve(sizeof(double) * (size_t)std::max(nsrc, 1) * K);
+        if (g->with_paths) b_ppath.reserve(sizeof(PathEnd) * (size_t)std::max(nsrc, 1) * K);
+        PlainOut P{};
+        P.order = d_order;
+        P.nsrc = nsrc;
+        P.tails = b_tails.as<int32_t>();
+        P.adj = b_padj.as<int32_t>();
+        P.dist = b_pdist.as<double>();
+        P.path = g->with_paths ? b_ppath.as<PathEnd>() : nullptr;
+        P.stats = O;
+        k_ich_plain<<<blocks, tpb, 0, st>>>(C, P);
+        ++launches;
+        SVG_CUDA(cudaGetLastError());
+        SVG_CUDA(cudaMemcpyAsync(&retry_n, d_retry_n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SVG_CUDA(cudaStreamSynchronize(st));
+        if (retry_n > 0)
+            throw SvgError{SVG_ERR_NOMEM, "plain build: a source outgrew its hash tables (raise K-based sizes)"};
+    } else {
+        int64_t cap = (int64_t)std::max(nsrc, 1) * ((int64_t)K + 64);
+        for (int attempt = 0;; ++attempt) {
+            b_cand.reserve(sizeof(Cand) * (size_t)cap);
+            b_candstart.reserve(sizeof(int64_t) * ((size_t)nv + 1));
+            O.cand = b_cand.as<Cand>();
+            O.cand_cap = cap;
+            O.cand_start = b_candstart.as<int64_t>();
+            k_ich_batched<<<blocks, tpb, 0, st>>>(C, O);
+            ++launches;
+            SVG_CUDA(cudaGetLastError());
+            SVG_CUDA(cudaMemcpyAsync(&retry_n, d_retry_n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            unsigned long long used = 0;
+            SVG_CUDA(cudaMemcpyAsync(&used, d_cand_used, sizeof(used), cudaMemcpyDeviceToHost, st));
+            SVG_CUDA(cudaStreamSynchronize(st));
+            if (retry_n > 0) {
+                // Sources whose tables filled: rerun them with 2x vertex and 4x split tables.
+                LaneConfig C2 = C;
+                Layout l2 = lay;
+                l2.vcap_log2 = retry_host_cap_log2_v;
+                l2.scap_log2 = retry_host_cap_log2_s;
+                l2.vlimit = (int32_t)(((int64_t)3 << l2.vcap_log2) / 4);
+                C2.vcap_log2 = l2.vcap_log2;
+                C2.scap_log2 = l2.scap_log2;
+                C2.vlimit = l2.vlimit;
+                C2.slimit = (int32_t)(((int64_t)3 << l2.scap_log2) / 4);
+                int tb2 = 64;
+                int bl2 = (int)std::min<int64_t>((retry_n + tb2 - 1) / tb2, (int64_t)prop.multiProcessorCount * 4);
+                l2.lanes = bl2 * tb2;
+                while (l2.lanes > 32 && (int64_t)(lane_bytes(l2) * l2.lanes) > budget) {
+                    bl2 = std::max(1, bl2 / 2);
+                    l2.lanes = bl2 * tb2;
+                }
+                carve(g_arena[1], l2, C2, st);
+                scratch_bytes += (int64_t)(lane_bytes(l2) * l2.lanes);
+                PhaseOut O2 = O;
+                O2.order = d_retry;
+                O2.nsrc = retry_n;
+                O2.work = d_work + 2;  // fresh queue head
+                O2.retry = d_retry + retry_n;  // a second failure lands after the first list
+                O2.retry_n = d_work + 3;
+                SVG_CUDA(cudaMemsetAsync(d_work + 2, 0, 2 * sizeof(int32_t), st));
+                k_ich_batched<<<bl2, tb2, 0, st>>>(C2, O2);
+                ++launches;
+                SVG_CUDA(cudaGetLastError());
+                int32_t again = 0;
+                SVG_CUDA(cudaMemcpyAsync(&again, d_work + 3, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+                SVG_CUDA(cudaMemcpyAsync(&used, d_cand_used, sizeof(used), cudaMemcpyDeviceToHost, st));
+                SVG_CUDA(cudaStreamSynchronize(st));
+                if (again > 0)
+                    throw SvgError{SVG_ERR_NOMEM, "a source outgrew the enlarged retry tables"};
+                smax_vlimit = std::max(smax_vlimit, l2.vlimit);
+            }
+            if ((int64_t)used <= cap) break;
+            if (attempt >= 2) throw SvgError{SVG_ERR_NOMEM, "candidate pool kept overflowing"};
+            cap = (int64_t)((double)used * 1.25) + 1024;
+            SVG_CUDA(cudaMemsetAsync(b_misc.p, 0, misc_bytes, st));
+            SVG_CUDA(cudaMemsetAsync(g->st_windows, 0, sizeof(int32_t) * (size_t)nv * 3, st));
+        }
+    }
+    SVG_CUDA(cudaEventRecord(ev[1], st));
+
+    // offsets = exclusive scan of degrees (vertices outside the range have 0)
+    size_t tmp_bytes = 0;
+    SVG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_deg, g->off, nv + 1, st));
+    DevBuf b_tmp;
+    b_tmp.reserve(tmp_bytes + 16);
+    // d_deg[nv] is zero: the scan over nv+1 entries leaves the edge total in off[nv]
+    SVG_CUDA(cub::DeviceScan::ExclusiveSum(b_tmp.p, tmp_bytes, d_deg, g->off, nv + 1, st));
+    ++launches;
+    int64_t nnz = 0;
+    SVG_CUDA(cudaMemcpyAsync(&nnz, g->off + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    g->nnz = nnz;
+    SVG_CUDA(cudaMalloc(&g->adj, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
+    SVG_CUDA(cudaMalloc(&g->dist, sizeof(double) * (size_t)std::max<int64_t>(nnz, 1)));
+    if (g->with_paths) SVG_CUDA(cudaMalloc(&g->paths, sizeof(PathEnd) * (size_t)std::max<int64_t>(nnz, 1)));
+    SVG_CUDA(cudaEventRecord(ev[2], st));
+
+    if (plain) {
+        k_compact<<<std::max(1, std::min(65535, (nsrc + 7) / 8)), 256, 0, st>>>(
+            d_order, nsrc, K, b_tails.as<int32_t>(), b_padj.as<int32_t>(), b_pdist.as<double>(),
+            g->with_paths ? b_ppath.as<PathEnd>() : nullptr, g->off, g->adj, g->dist,
+            reinterpret_cast<PathEnd*>(g->paths));
+        ++launches;
+    } else if (nsrc > 0) {
+        EmitParams E{};
+        E.M = C.M;
+        E.K = K;
+        E.nv = nv;
+        E.order = d_order;
+        E.nsrc = nsrc;
+        E.cand = b_cand.as<Cand>();
+        E.cand_start = b_candstart.as<int64_t>();
+        E.cand_n = d_cand_n;
+        E.off = g->off;
+        E.adj = g->adj;
+        E.dist = g->dist;
+        E.path = reinterpret_cast<PathEnd*>(g->paths);
+        E.st_flags = g->st_flags;
+        int smax = 32;
+        while (smax < smax_vlimit) smax <<= 1;
+        E.smax = smax;
+        int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / ((int64_t)smax * 8)));
+        size_t smem = (size_t)wpb * smax * 8;
+        SVG_CUDA(cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int eb = (int)std::min<int64_t>((nsrc + wpb - 1) / wpb, (int64_t)prop.multiProcessorCount * 16);
+        k_emit<<<eb, wpb * 32, smem, st>>>(E);
+        ++launches;
+    }
+    SVG_CUDA(cudaGetLastError());
+    SVG_CUDA(cudaEventRecord(ev[3], st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+
+    unsigned long long acc[8] = {0};
+    SVG_CUDA(cudaMemcpy(acc, d_acc, sizeof(acc), cudaMemcpyDeviceToHost));
+    float t01 = 0, t23 = 0, t03 = 0;
+    SVG_CUDA(cudaEventElapsedTime(&t01, ev[0], ev[1]));
+    SVG_CUDA(cudaEventElapsedTime(&t23, ev[2], ev[3]));
+    SVG_CUDA(cudaEventElapsedTime(&t03, ev[0], ev[3]));
+    for (auto& e : ev) cudaEventDestroy(e);
+
+    svg_build_stats& S = g->stats;
+    S = svg_build_stats{};
+    S.ms_ich = t01;
+    S.ms_emit = t23;
+    S.ms_total = t01 + t23;  // excludes the host-side CSR allocation between the phases
+    S.windows = (int64_t)acc[0];
+    S.windows_generated = (int64_t)acc[1];
+    S.pseudo_sources = (int64_t)acc[2];
+    S.max_win_queue = (int32_t)acc[3];
+    S.max_pseudo_queue = (int32_t)acc[4];
+    S.edges = nnz;
+    S.sources = nsrc;
+    S.retried_sources = retry_n;
+    S.launches = launches;
+    S.scratch_bytes = scratch_bytes;
+    (void)t03;
+    // flag tallies
+    std::vector<int32_t> fl((size_t)nv);
+    SVG_CUDA(cudaMemcpy(fl.data(), g->st_flags, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
+    for (int32_t f : fl) {
+        if (f & 1) ++S.queue_drop_sources;
+        if (f & 2) ++S.ref_overflow_sources;
+        if (f & 4) ++S.watchdog_sources;
+        if (f & 8) ++S.undefined_sources;
+    }
+    return SVG_OK;
+}
+
+}  // namespace svgb

@@ -1,0 +1,87 @@
+// Library objects and host-side helpers shared by the C-ABI and the kernels' launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "svg_b200.h"
+#include "svg_internal.h"
+
+namespace svgb {
+
+void set_error(const std::string& msg);
+
+struct CudaFail {
+    cudaError_t err;
+    std::string where;
+};
+
+#define SVG_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess) throw ::svgb::CudaFail{e__, std::string(#call) + " @ " + __FILE__ + ":" + std::to_string(__LINE__)}; \
+    } while (0)
+
+struct SvgError {
+    svg_status code;
+    std::string msg;
+};
+
+// The library's CUDA stream and events (one device: the current one at first use).
+cudaStream_t lib_stream();
+
+// Growable device buffer, reused across calls.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n);   // grows (contents not preserved)
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(p); }
+    ~DevBuf() { release(); }
+};
+
+struct MeshDev {
+    bool uploaded = false;
+    HeRec* he = nullptr;
+    HeGeo* geo = nullptr;
+    VertRec* vr = nullptr;
+    double* pos = nullptr;
+    DevMesh view() const;
+};
+
+}  // namespace svgb
+
+struct svg_mesh {
+    svgb::HostMesh h;
+    svgb::MeshDev d;
+};
+
+struct svg_graph {
+    svg_mesh* mesh = nullptr;
+    int32_t K = 0;
+    int32_t nv = 0;
+    int64_t nnz = 0;
+    bool with_paths = false;
+    int64_t* off = nullptr;        // nv+1
+    int32_t* adj = nullptr;        // nnz
+    double* dist = nullptr;        // nnz
+    void* paths = nullptr;         // nnz PathEnd (optional)
+    int32_t* st_windows = nullptr; // nv per-source counters (device)
+    int32_t* st_maxq = nullptr;
+    int32_t* st_flags = nullptr;
+    svg_build_stats stats{};
+    // query scratch
+    svgb::DevBuf qbuf;
+};
+
+namespace svgb {
+svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g);
+void upload_mesh(svg_mesh* m);
+void free_graph_device(svg_graph* g);
+svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist);
+svg_status run_msad(svg_graph* g, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w,
+                    double* d_dist, int32_t* d_src_id, int64_t total_srcs);
+}  // namespace svgb

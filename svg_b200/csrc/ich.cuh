@@ -1,0 +1,760 @@
+// Device ICH engine: one K-limited Improved-Chen-Han window propagation per
+// lane, the reference's algorithm (ICHDevice.cu) step for step.
+//
+// Arithmetic: every expression that decides a branch or produces an output
+// is the reference's, in the reference's operation order; the library is
+// compiled with --fmad=false so nothing is contracted into an FMA.  Values
+// that depend only on the mesh (corner angles, unfolded apex positions) are
+// precomputed on the host with the same formulas and read here.
+//
+// Per-lane state lives in global memory (L1/L2-cached), sized per lane:
+//   window heap : 16-byte {key, psrc, slot|birth} entries, 1-based binary
+//                 min-heap with the reference's sift rules
+//                 (PriorityQueue.cuh:48-105), interleaved across the 32 lanes
+//                 of a warp so index i of all lanes is one 512-byte span;
+//   window pool : 48-byte payloads addressed by slot, recycled via a stack;
+//   pseudo heap : 16-byte {key, vert, level<<8|birth} entries, same heap;
+//   vertex table: 32-byte slots, open addressing, epoch-stamped (no clears);
+//   split table : 32-byte slots, same scheme;
+//   vertex list : keys in insertion order (the emission walks only these).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "svg_internal.h"
+
+namespace svgb {
+
+constexpr double kRefPi = 3.141592653589793238;  // Geometry.cuh:18
+constexpr double kRelErr = 1e-8;                  // ICHDevice.cuh:10
+
+// per-source flags
+enum : int32_t {
+    kFlagQueueDrop = 1,     // a push found its queue full and was dropped (reference behaviour)
+    kFlagRefOverflow = 2,   // the reference's fixed-size hash table would have overflowed
+    kFlagWatchdog = 4,      // an iteration cap stopped a loop the reference could spin in
+    kFlagUndefined = 8,     // a step the reference leaves undefined (edges[-1])
+    kFlagCapacity = 16,     // this lane's tables filled: the source is re-run with bigger ones
+};
+
+struct alignas(16) WinEntry {
+    double key;     // window minDist
+    int32_t psrc;   // pseudo-source vertex
+    uint32_t sb;    // pool slot (low 16 bits) | birth (bits 16..23)
+};
+struct alignas(16) WinPay {
+    double b0, b1;  // interval on the half-edge
+    double sx, sy;  // unfolded (pseudo-)source, FlatenedSrc (ICHDevice.cuh:41-49)
+    double psd;     // pseudoSrcDist
+    int32_t edge;
+    int32_t level;
+};
+struct alignas(16) PsEntry {
+    double key;     // pseudo-source distance
+    int32_t vert;
+    uint32_t lb;    // level << 8 | birth
+};
+struct alignas(32) VSlot {
+    uint32_t key;
+    uint32_t epoch;
+    int32_t enter;  // enterEdge
+    int32_t birth;  // char birthTime, sign-extended
+    double dist;
+    double pad;
+};
+struct alignas(32) SSlot {
+    uint32_t key;
+    uint32_t epoch;
+    int32_t psrc;   // pseudoSrcId
+    int32_t pad;
+    double dist;
+    double x;
+};
+
+// A direct SVG candidate produced by the propagation phase.
+struct alignas(8) Cand {
+    int32_t u;      // vertex
+    int32_t ee;     // enterEdge (edge key point), -1 = no interior key point
+    double dist;
+    double x;       // splitInfos[ee].x
+};
+
+// Path ends of an SVG edge (SVGNode fields other than adj/dist).
+struct alignas(8) PathEnd {
+    uint32_t src_edge, dst_edge;
+    double src_x, dst_x;
+};
+
+struct LaneConfig {
+    DevMesh M;
+    int32_t K;
+    int32_t wcap, pcap;      // queue capacities (logical = physical)
+    uint32_t vref, sref;     // the reference's table sizes, K*vert_coef and K*split_coef
+    int32_t vcap_log2, scap_log2;
+    int32_t vlimit, slimit;  // max keys this lane's tables take before kFlagCapacity
+    int64_t watchdog;        // max steps per source
+    WinEntry* wheap;
+    WinPay* wpool;
+    uint16_t* wfree;
+    PsEntry* pheap;
+    VSlot* vtab;
+    int32_t* vlist;
+    SSlot* stab;
+    uint32_t* epochs;
+};
+
+__device__ __forceinline__ int nxt(int e) { return (e % 3 == 2) ? e - 2 : e + 1; }
+__device__ __forceinline__ int prv(int e) { return (e % 3 == 0) ? e + 2 : e - 1; }
+
+__device__ __forceinline__ HeRec ld_he(const HeRec* p, int e) {
+    const int4* q = reinterpret_cast<const int4*>(p + e);
+    int4 a = __ldg(q);
+    int4 b = __ldg(q + 1);
+    HeRec h;
+    h.v0 = a.x; h.v1 = a.y; h.twin = a.z; h.pad = a.w;
+    h.len = __hiloint2double(b.y, b.x);
+    h.corner = __hiloint2double(b.w, b.z);
+    return h;
+}
+__device__ __forceinline__ double2 ld_apex(const HeGeo* g, int e) {
+    return __ldg(reinterpret_cast<const double2*>(g + e));
+}
+__device__ __forceinline__ double2 ld_top(const HeGeo* g, int e) {
+    return __ldg(reinterpret_cast<const double2*>(g + e) + 1);
+}
+
+// ICHDevice::Intersect (ICHDevice.cu:975-980)
+__device__ __forceinline__ double isect(double v0x, double v0y, double v1x, double v1y, double p0x, double p0y,
+                                        double p1x, double p1y) {
+    double a00 = p0x - p1x, a01 = v1x - v0x, b0 = v1x - p1x;
+    double a10 = p0y - p1y, a11 = v1y - v0y, b1 = v1y - p1y;
+    return (b0 * a11 - b1 * a01) / (a00 * a11 - a10 * a01);
+}
+__device__ __forceinline__ double hyp(double x, double y) { return sqrt(x * x + y * y); }
+
+// toLeft (Geometry.cu:306-310) with Vector2D::normalize (Geometry.cuh:35)
+__device__ __forceinline__ bool to_left(double px, double py, double p0x, double p0y, double p1x, double p1y) {
+    double ax = p1x - p0x, ay = p1y - p0y;
+    double bx = px - p0x, by = py - p0y;
+    double la = sqrt(ax * ax + ay * ay);
+    if (!(fabs(la) < 1e-12)) { ax /= la; ay /= la; }
+    double lb = sqrt(bx * bx + by * by);
+    if (!(fabs(lb) < 1e-12)) { bx /= lb; by /= lb; }
+    return (ax * by - ay * bx) > 0.0;
+}
+
+// A window being built: Window::calcMinDist + FlatenedSrc (ICHDevice.cuh:30-49)
+// share xProj = (d0^2 + wLen^2 - d1^2) / (2 wLen).
+struct NewWin {
+    double key;
+    WinPay p;
+};
+__device__ __forceinline__ void finish_window(double b0, double b1, double d0, double d1, double psd, NewWin& w) {
+    double wLen = b1 - b0;
+    double xProj = (d0 * d0 + wLen * wLen - d1 * d1) / (2 * wLen);
+    double h = sqrt(fabs(d0 * d0 - xProj * xProj));
+    if (xProj < 0.0) w.key = d0 + psd;
+    else if (xProj > wLen) w.key = d1 + psd;
+    else w.key = h + psd;
+    w.p.b0 = b0;
+    w.p.b1 = b1;
+    w.p.sx = xProj + b0;
+    w.p.sy = h;
+    w.p.psd = psd;
+}
+
+struct Lane {
+    const LaneConfig& C;
+    WinEntry* WH;   // this lane's heap column (stride 32 entries)
+    PsEntry* PH;
+    WinPay* WP;
+    uint16_t* WF;
+    VSlot* VT;
+    int32_t* VL;
+    SSlot* ST;
+    int wsize, psize, nfree, nfresh;
+    int vcount, scount;
+    uint32_t epoch;
+    int source;
+    int src_birth;
+    int total;      // totalCalcVertNum
+    int flags;
+    int windows, pseudos, generated, maxw, maxp;
+    int64_t steps;
+
+    __device__ Lane(const LaneConfig& c, int gtid) : C(c) {
+        int warp = gtid >> 5, lane = gtid & 31;
+        WH = C.wheap + (size_t)warp * (C.wcap + 1) * 32 + lane;
+        PH = C.pheap + (size_t)warp * (C.pcap + 1) * 32 + lane;
+        WP = C.wpool + (size_t)gtid * C.wcap;
+        WF = C.wfree + (size_t)gtid * C.wcap;
+        VT = C.vtab + ((size_t)gtid << C.vcap_log2);
+        VL = C.vlist + (size_t)gtid * C.vlimit;
+        ST = C.stab + ((size_t)gtid << C.scap_log2);
+        epoch = C.epochs[gtid];
+    }
+
+    __device__ __forceinline__ WinEntry& wh(int i) { return WH[(size_t)i << 5]; }
+    __device__ __forceinline__ PsEntry& ph(int i) { return PH[(size_t)i << 5]; }
+
+    // ---------------------------------------------------------- tables
+    __device__ __forceinline__ uint32_t vhash(uint32_t k) const { return (k * 0x9E3779B1u) >> (32 - C.vcap_log2); }
+    __device__ __forceinline__ uint32_t shash(uint32_t k) const { return (k * 0x9E3779B1u) >> (32 - C.scap_log2); }
+
+    // slot index of vertex v, or -1 if absent
+    __device__ __forceinline__ int vfind(int v) {
+        uint32_t mask = (1u << C.vcap_log2) - 1, h = vhash((uint32_t)v);
+        for (;;) {
+            uint2 ke = *reinterpret_cast<const uint2*>(&VT[h]);
+            if (ke.y != epoch) return -1;
+            if (ke.x == (uint32_t)v) return (int)h;
+            h = (h + 1) & mask;
+        }
+    }
+    __device__ __forceinline__ double vdist(int v) {
+        int s = vfind(v);
+        return s < 0 ? DBL_MAX : VT[s].dist;
+    }
+    __device__ __forceinline__ int vbirth(int v) {
+        int s = vfind(v);
+        return s < 0 ? -1 : VT[s].birth;
+    }
+    // MyHashTable::operator[] (MyHashTable.cuh:72-82): find or insert with defaults
+    __device__ int vput(int v) {
+        uint32_t mask = (1u << C.vcap_log2) - 1, h = vhash((uint32_t)v);
+        for (;;) {
+            uint2 ke = *reinterpret_cast<const uint2*>(&VT[h]);
+            if (ke.y != epoch) break;
+            if (ke.x == (uint32_t)v) return (int)h;
+            h = (h + 1) & mask;
+        }
+        if (vcount >= C.vlimit) {  // keep the probe chains short: hand the source to the big pass
+            flags |= kFlagCapacity;
+            return -1;
+        }
+        VSlot s;
+        s.key = (uint32_t)v; s.epoch = epoch; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.pad = 0.0;
+        VT[h] = s;
+        VL[vcount] = v;
+        ++vcount;
+        if ((uint32_t)vcount > C.vref) flags |= kFlagRefOverflow;
+        return (int)h;
+    }
+    __device__ __forceinline__ int sfind(int e) {
+        uint32_t mask = (1u << C.scap_log2) - 1, h = shash((uint32_t)e);
+        for (;;) {
+            uint2 ke = *reinterpret_cast<const uint2*>(&ST[h]);
+            if (ke.y != epoch) return -1;
+            if (ke.x == (uint32_t)e) return (int)h;
+            h = (h + 1) & mask;
+        }
+    }
+    __device__ int sput(int e) {
+        uint32_t mask = (1u << C.scap_log2) - 1, h = shash((uint32_t)e);
+        for (;;) {
+            uint2 ke = *reinterpret_cast<const uint2*>(&ST[h]);
+            if (ke.y != epoch) break;
+            if (ke.x == (uint32_t)e) return (int)h;
+            h = (h + 1) & mask;
+        }
+        if (scount >= C.slimit) {
+            flags |= kFlagCapacity;
+            return -1;
+        }
+        SSlot s;
+        s.key = (uint32_t)e; s.epoch = epoch; s.psrc = -1; s.pad = 0; s.dist = DBL_MAX; s.x = DBL_MAX;
+        ST[h] = s;
+        ++scount;
+        if ((uint32_t)scount > C.sref) flags |= kFlagRefOverflow;
+        return (int)h;
+    }
+    // Reset every slot (the plain build's per-source Clear, ICHDevice.cu:487-523).
+    __device__ void clear_tables() {
+        for (int i = 0; i < (1 << C.vcap_log2); ++i) {
+            VSlot s;
+            s.key = 0xFFFFFFFFu; s.epoch = 0; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.pad = 0.0;
+            VT[i] = s;
+        }
+        for (int i = 0; i < (1 << C.scap_log2); ++i) {
+            SSlot s;
+            s.key = 0xFFFFFFFFu; s.epoch = 0; s.psrc = -1; s.pad = 0; s.dist = DBL_MAX; s.x = DBL_MAX;
+            ST[i] = s;
+        }
+    }
+
+    // ----------------------------------------------------------- heaps
+    __device__ void wpush(const NewWin& w, int psrc, int birth) {
+        ++generated;  // counts attempts, like numOfWinGen
+        if (wsize >= C.wcap) {  // PriorityQueue.cuh:53: dropped when full
+            flags |= kFlagQueueDrop;
+            return;
+        }
+        int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
+        WP[slot] = w.p;
+        int cur = ++wsize, p = cur >> 1;
+        while (p > 0) {
+            WinEntry pe = wh(p);
+            if (!(pe.key > w.key)) break;
+            wh(cur) = pe;
+            cur = p;
+            p = cur >> 1;
+        }
+        WinEntry e;
+        e.key = w.key; e.psrc = psrc; e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
+        wh(cur) = e;
+        if (wsize > maxw) maxw = wsize;
+    }
+    __device__ WinEntry wpop() {
+        WinEntry top = wh(1);
+        WinEntry last = wh(wsize);
+        --wsize;
+        int cur = 1;
+        for (;;) {
+            int l = cur << 1, r = l + 1, mc;
+            WinEntry ce;
+            if (r <= wsize) {
+                WinEntry a = wh(l), b = wh(r);
+                if (a.key < b.key) { mc = l; ce = a; } else { mc = r; ce = b; }
+            } else if (l <= wsize) {
+                mc = l; ce = wh(l);
+            } else {
+                break;
+            }
+            if (!(ce.key < last.key)) break;
+            wh(cur) = ce;
+            cur = mc;
+        }
+        wh(cur) = last;
+        WF[nfree++] = (uint16_t)(top.sb & 0xFFFF);
+        return top;
+    }
+    __device__ void ppush(double key, int vert, int level, int birth) {
+        if (psize >= C.pcap) {
+            flags |= kFlagQueueDrop;
+            return;
+        }
+        int cur = ++psize, p = cur >> 1;
+        while (p > 0) {
+            PsEntry pe = ph(p);
+            if (!(pe.key > key)) break;
+            ph(cur) = pe;
+            cur = p;
+            p = cur >> 1;
+        }
+        PsEntry e;
+        e.key = key; e.vert = vert; e.lb = ((uint32_t)level << 8) | (uint32_t)(birth & 0xFF);
+        ph(cur) = e;
+        if (psize > maxp) maxp = psize;
+    }
+    __device__ PsEntry ppop() {
+        PsEntry top = ph(1);
+        PsEntry last = ph(psize);
+        --psize;
+        int cur = 1;
+        for (;;) {
+            int l = cur << 1, r = l + 1, mc;
+            PsEntry ce;
+            if (r <= psize) {
+                PsEntry a = ph(l), b = ph(r);
+                if (a.key < b.key) { mc = l; ce = a; } else { mc = r; ce = b; }
+            } else if (l <= psize) {
+                mc = l; ce = ph(l);
+            } else {
+                break;
+            }
+            if (!(ce.key < last.key)) break;
+            ph(cur) = ce;
+            cur = mc;
+        }
+        ph(cur) = last;
+        return top;
+    }
+
+    // -------------------------------------------------- source lifecycle
+    __device__ void begin(int v, bool clear_all) {
+        source = v;
+        wsize = psize = nfree = nfresh = 0;
+        vcount = scount = 0;
+        total = 0;
+        flags = 0;
+        windows = pseudos = generated = maxw = maxp = 0;
+        steps = 0;
+        src_birth = 0;
+        if (clear_all) {
+            clear_tables();  // every slot now carries epoch 0 = empty
+            epoch = 1;
+        } else {
+            ++epoch;
+            if (epoch == 0) ++epoch;
+        }
+        initialize();
+    }
+    __device__ void save_epoch(int gtid) { C.epochs[gtid] = epoch; }
+
+    // write the birth of vertex slot s, keeping the source's cached birth
+    __device__ __forceinline__ void set_birth(int s, int v, int b) {
+        VT[s].birth = b;
+        if (v == source) src_birth = b;
+    }
+
+    // ICHDevice::Initialize, vertex source (ICHDevice.cu:525-581)
+    __device__ void initialize() {
+        const DevMesh& M = C.M;
+        int start = __ldg(&M.vr[source].first);
+        if (start < 0) {  // isolated vertex: the reference indexes edges[-1]
+            flags |= kFlagUndefined;
+            return;
+        }
+        int cur = start;
+        int guard = 0;
+        do {
+            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
+            HeRec hc = ld_he(M.he, cur);
+            int op = nxt(cur);
+            HeRec ho = ld_he(M.he, op);
+            HeRec hp = ld_he(M.he, prv(cur));
+            NewWin w;
+            finish_window(0.0, ho.len, hc.len, hp.len, 0.0, w);
+            w.p.edge = op;
+            w.p.level = 0;
+            wpush(w, source, 0);
+            int opv = hc.v1;
+            int s = vput(opv);
+            if (s < 0) return;
+            if (hc.len > VT[s].dist) {
+                cur = hc.twin;
+                if (cur != -1) cur = nxt(cur);
+                continue;
+            }
+            set_birth(s, opv, 0);
+            VT[s].dist = hc.len;
+            VT[s].enter = hc.twin;
+            if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE)) {
+                cur = hc.twin;
+                if (cur != -1) cur = nxt(cur);
+                continue;
+            }
+            ppush(hc.len, opv, 0, VT[s].birth);
+            cur = hc.twin;
+            if (cur != -1) cur = nxt(cur);
+        } while (cur != start && cur != -1);
+        int s = vput(source);
+        if (s < 0) return;
+        set_birth(s, source, 0);
+        VT[s].dist = 0.0;
+        VT[s].enter = -1;
+    }
+
+    // ICHDevice::IsValidWindow (ICHDevice.cu:906-955).  v1, v2, v3: start,
+    // end and opposite vertex of the window's half-edge; l0 its length;
+    // (tx,ty) the opposite vertex in the window's frame.
+    __device__ bool is_valid(const NewWin& w, bool isLeft, int v1, int v2, int v3, double l0, double tx, double ty) {
+        const WinPay& p = w.p;
+        if (p.b1 <= p.b0) return false;
+        double dB = hyp(p.sx - p.b1, p.sy - 0.0);
+        double dA = hyp(p.sx - p.b0, p.sy - 0.0);
+        double d1 = vdist(v1);
+        if (p.psd + dB > d1 + p.b1 && (p.psd + dB) / (d1 + p.b1) - 1.0 > 0.0) return false;
+        double d2 = vdist(v2);
+        if (p.psd + dA > d2 + l0 - p.b0 && (p.psd + dA) / (d2 + l0 - p.b0) - 1.0 > 0.0) return false;
+        double d3 = vdist(v3);
+        if (isLeft) {
+            double q = hyp(tx - p.b0, ty - 0.0);
+            if (p.psd + dA > d3 + q && (p.psd + dA) / (d3 + q) - 1.0 > 0.0) return false;
+        } else {
+            double q = hyp(tx - p.b1, ty - 0.0);
+            if (p.psd + dB > d3 + q && (p.psd + dB) / (d3 + q) - 1.0 > kRelErr) return false;
+        }
+        return true;
+    }
+
+    // ICHDevice::BuildWindow (ICHDevice.cu:957-973)
+    __device__ __forceinline__ void build_window(const WinPay& f, int edge, double elen, double t0, double t1,
+                                                 double v0x, double v0y, double v1x, double v1y, NewWin& w) {
+        double b0 = (1 - t0) * elen, b1 = (1 - t1) * elen;
+        double px = v0x * t0 + v1x * (1 - t0), py = v0y * t0 + v1y * (1 - t0);
+        double d0 = hyp(f.sx - px, f.sy - py);
+        px = v0x * t1 + v1x * (1 - t1);
+        py = v0y * t1 + v1y * (1 - t1);
+        double d1 = hyp(f.sx - px, f.sy - py);
+        finish_window(b0, b1, d0, d1, f.psd, w);
+        w.p.edge = edge;
+        w.p.level = f.level + 1;
+    }
+
+    // ICHDevice::PropagateWindow (ICHDevice.cu:618-726)
+    __device__ void propagate(const WinPay& win, int psrc, int birth) {
+        const DevMesh& M = C.M;
+        int e0 = ld_he(M.he, win.edge).twin;
+        if (e0 == -1) return;
+        int e1 = nxt(e0), e2 = nxt(e1);
+        HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
+        int opv = h1.v1;
+        double sx = win.sx, sy = win.sy;
+        double l0 = h0.len;
+        double2 v2 = ld_apex(M.geo, e0);
+        double interX = v2.x - v2.y * (v2.x - sx) / (v2.y - sy);
+        NewWin L, R;
+        bool hasL = true, hasR = true;
+        if (interX <= win.b0) {
+            hasL = false;
+            double t0 = isect(sx, sy, win.b0, 0.0, v2.x, v2.y, l0, 0.0);
+            double t1 = isect(sx, sy, win.b1, 0.0, v2.x, v2.y, l0, 0.0);
+            build_window(win, e2, h2.len, t0, t1, v2.x, v2.y, l0, 0.0, R);
+            double2 tp = ld_top(M.geo, e2);
+            if (!is_valid(R, false, h2.v0, h2.v1, h0.v1, h2.len, tp.x, tp.y)) hasR = false;
+        } else if (interX >= win.b1) {
+            hasR = false;
+            double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
+            double t1 = isect(sx, sy, win.b1, 0.0, 0.0, 0.0, v2.x, v2.y);
+            build_window(win, e1, h1.len, t0, t1, 0.0, 0.0, v2.x, v2.y, L);
+            double2 tp = ld_top(M.geo, e1);
+            if (!is_valid(L, true, h1.v0, h1.v1, h0.v0, h1.len, tp.x, tp.y)) hasL = false;
+        } else {
+            double direct = hyp(v2.x - sx, v2.y - sy);
+            double D = direct + win.psd;
+            int ss = sfind(e0);
+            double sd = ss < 0 ? DBL_MAX : ST[ss].dist;
+            if (D > sd && D / sd - 1.0 > kRelErr) {  // one angle, one split
+                hasL = (ss < 0 ? DBL_MAX : ST[ss].x) < interX;
+                hasR = !hasL;
+            } else {
+                if (D < sd) {
+                    int s = sput(e0);
+                    if (s < 0) return;
+                    ST[s].dist = D;
+                    ST[s].psrc = psrc;
+                    ST[s].x = l0 - interX;
+                }
+                int vs = vfind(opv);
+                double vd = vs < 0 ? DBL_MAX : VT[vs].dist;
+                if (D < vd) {
+                    if (vd == DBL_MAX) ++total;
+                    int s = vs < 0 ? vput(opv) : vs;
+                    if (s < 0) return;
+                    int b = (int)(signed char)(VT[s].birth + 1);
+                    set_birth(s, opv, b);
+                    VT[s].dist = D;
+                    VT[s].enter = e0;
+                    if (__ldg(&M.vr[opv].flags) & kVertSaddleGT) ppush(D, opv, win.level + 1, b);
+                }
+            }
+            if (hasL) {
+                double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
+                build_window(win, e1, h1.len, t0, 0.0, 0.0, 0.0, v2.x, v2.y, L);
+                double2 tp = ld_top(M.geo, e1);
+                if (!is_valid(L, true, h1.v0, h1.v1, h0.v0, h1.len, tp.x, tp.y)) hasL = false;
+            }
+            if (hasR) {
+                double t1 = isect(sx, sy, win.b1, 0.0, v2.x, v2.y, l0, 0.0);
+                build_window(win, e2, h2.len, 1.0, t1, v2.x, v2.y, l0, 0.0, R);
+                double2 tp = ld_top(M.geo, e2);
+                if (!is_valid(R, false, h2.v0, h2.v1, h0.v1, h2.len, tp.x, tp.y)) hasR = false;
+            }
+        }
+        if (hasL) wpush(L, psrc, birth);
+        if (hasR) wpush(R, psrc, birth);
+    }
+
+    // Fan walks of GenSubWinsForPseudoSrcFrom{Window,PseudoSrc}
+    // (ICHDevice.cu:821-857, 867-903) with precomputed corner angles.
+    __device__ void fan_walk(int left, int right, double a0, double a1, int& startEdge, int& endEdge) {
+        const DevMesh& M = C.M;
+        startEdge = -1;
+        endEdge = -1;
+        int cur = left;
+        int guard = 0;
+        while (a0 < kRefPi && cur != -1) {
+            int nx = nxt(nxt(cur));
+            a0 += ld_he(M.he, cur).corner;
+            cur = ld_he(M.he, nx).twin;
+            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
+        }
+        if (cur != -1) startEdge = nxt(ld_he(M.he, cur).twin);
+        cur = right;
+        while (a1 < kRefPi && cur != -1) {
+            int nx = nxt(cur);
+            a1 += ld_he(M.he, nx).corner;
+            cur = ld_he(M.he, nx).twin;
+            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
+        }
+        if (cur != -1) endEdge = ld_he(M.he, nxt(nxt(ld_he(M.he, cur).twin))).twin;
+    }
+
+    // ICHDevice::GenSubWinsForPseudoSrc (ICHDevice.cu:728-793)
+    __device__ void gen_sub_wins(double pdist, int pv, int plevel, int pbirth) {
+        const DevMesh& M = C.M;
+        int vs = vfind(pv);
+        int enter = vs < 0 ? -1 : VT[vs].enter;
+        int vb = vs < 0 ? -1 : VT[vs].birth;
+        int startEdge, endEdge;
+        if (enter == -1 && vb != -1) {
+            startEdge = __ldg(&M.vr[pv].first);
+            endEdge = startEdge;
+        } else if (enter >= 0 && ld_he(M.he, enter).v0 == pv) {
+            fan_walk(enter, ld_he(M.he, enter).twin, 0.0, 0.0, startEdge, endEdge);
+        } else if (enter >= 0 && ld_he(M.he, nxt(enter)).v1 == pv) {
+            // GenSubWinsForPseudoSrcFromWindow (ICHDevice.cu:795-858)
+            int e0 = enter, e1 = nxt(e0), e2 = nxt(e1);
+            HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
+            double l0 = h0.len, l1 = h1.len, l2 = h2.len;
+            int ss = sfind(e0);
+            double sx = ss < 0 ? DBL_MAX : ST[ss].x;
+            double ex = l0 - sx, ey = 0.0;
+            double2 v2 = ld_apex(M.geo, e0);
+            double dx = ex - v2.x, dy = ey - v2.y;
+            double dl = hyp(dx, dy);
+            double a0 = (dx * (0.0 - v2.x) + dy * (0.0 - v2.y)) / dl / l1;
+            double a1 = (dx * (l0 - v2.x) + dy * (0.0 - v2.y)) / dl / l2;
+            if (a0 > 1.0) a0 = 1.0; else if (a0 < -1.0) a0 = -1.0;
+            if (a1 > 1.0) a1 = 1.0; else if (a1 < -1.0) a1 = -1.0;
+            a0 = acos(a0);
+            a1 = acos(a1);
+            fan_walk(h1.twin, h2.twin, a0, a1, startEdge, endEdge);
+        } else {
+            flags |= kFlagUndefined;  // assert(false) at ICHDevice.cu:740
+            return;
+        }
+        if (flags & kFlagWatchdog) return;
+        int guard = 0;
+        do {
+            if (startEdge < 0) {  // the reference reads edges[-1] here
+                flags |= kFlagUndefined;
+                break;
+            }
+            int we = nxt(startEdge);
+            HeRec hs = ld_he(M.he, startEdge), hw = ld_he(M.he, we);
+            HeRec hn = ld_he(M.he, nxt(we));
+            NewWin w;
+            finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
+            w.p.edge = we;
+            w.p.level = plevel + 1;
+            wpush(w, pv, pbirth);
+            startEdge = hn.twin;
+            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
+        } while (startEdge != endEdge);
+
+        int start = __ldg(&M.vr[pv].first), cur = start;
+        guard = 0;
+        do {
+            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
+            HeRec hc = ld_he(M.he, cur);
+            int opv = hc.v1;
+            int os = vfind(opv);
+            double od = os < 0 ? DBL_MAX : VT[os].dist;
+            if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE) || od < pdist + hc.len) {
+                cur = hc.twin;
+                if (cur != -1) cur = nxt(cur);
+                continue;
+            }
+            if (od == DBL_MAX) ++total;
+            int s = os < 0 ? vput(opv) : os;
+            if (s < 0) return;
+            VT[s].dist = pdist + hc.len;
+            int b = (int)(signed char)(VT[s].birth + 1);
+            set_birth(s, opv, b);
+            VT[s].enter = hc.twin;
+            ppush(VT[s].dist, opv, plevel, b);
+            cur = hc.twin;
+            if (cur != -1) cur = nxt(cur);
+        } while (cur != start && cur != -1);
+    }
+
+    // One iteration of ICHDevice::Execute's loop (ICHDevice.cu:72-119).
+    // Returns true when the source is finished.
+    __device__ bool step() {
+        if (wsize == 0 && psize == 0) return true;
+        if (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined)) return true;
+        if (++steps > C.watchdog) {
+            flags |= kFlagWatchdog;
+            return true;
+        }
+        // stale tops: birth no longer matches the pseudo-source's
+        while (wsize > 0) {
+            WinEntry t = wh(1);
+            int b = (t.psrc == source) ? src_birth : vbirth(t.psrc);
+            if ((int)(signed char)(t.sb >> 16) == b) break;
+            wpop();
+        }
+        while (psize > 0) {
+            PsEntry t = ph(1);
+            if ((int)(signed char)(t.lb & 0xFF) == vbirth(t.vert)) break;
+            ppop();
+        }
+        double wk = wsize > 0 ? wh(1).key : 0.0;
+        double pk = psize > 0 ? ph(1).key : 0.0;
+        if (wsize > 0 && (psize == 0 || wk < pk)) {
+            WinEntry t = wpop();
+            WinPay p = WP[t.sb & 0xFFFF];
+            if (p.level > C.M.nf) return false;
+            ++windows;
+            propagate(p, t.psrc, (int)(signed char)(t.sb >> 16));
+        } else if (psize > 0 && (wsize == 0 || wk >= pk)) {
+            PsEntry t = ppop();
+            int level = (int)(t.lb >> 8);
+            if (level >= C.M.nf) return false;
+            ++pseudos;
+            gen_sub_wins(t.key, t.vert, level, (int)(signed char)(t.lb & 0xFF));
+        } else if (wsize > 0 || psize > 0) {
+            flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
+            return true;
+        } else {
+            return true;
+        }
+        if (C.K != -1 && total >= C.K) return true;
+        return false;
+    }
+};
+
+// ICHDevice::BuildGeodesicPathTo(vertex) (ICHDevice.cu:336-480) for a
+// vertex whose path reaches the source through windows only: walk back from
+// key point (ee, x) across faces until the source is the opposite vertex.
+// Outputs the last key point (next to the source); -1 if there is none.
+__device__ __forceinline__ void trace_direct(const DevMesh& M, int source, int ee, double x, uint32_t& src_edge,
+                                             double& src_x, int& flags) {
+    src_edge = 0xFFFFFFFFu;
+    src_x = 0.0;
+    int gid = ee;
+    double gpos = x;
+    HeRec hg = ld_he(M.he, gid);
+    if (hg.twin < 0) { flags |= kFlagUndefined; return; }
+    int opv = ld_he(M.he, nxt(hg.twin)).v1;
+    double2 last = ld_apex(M.geo, gid);
+    double cx = hg.len - gpos, cy = 0.0;
+    int guard = 0;
+    while (opv != source) {
+        if (++guard > M.nf + 8) { flags |= kFlagWatchdog; return; }
+        int e0 = hg.twin, e1 = nxt(e0), e2 = nxt(e1);
+        double L0 = ld_he(M.he, e0).len, L1 = ld_he(M.he, e1).len, L2 = ld_he(M.he, e2).len;
+        double2 ov = ld_top(M.geo, e0);
+        double s = gpos / L0, t = 1.0 - gpos / L0;
+        double2 nl;
+        if (to_left(ov.x, ov.y, last.x, last.y, cx, cy)) {
+            double2 p0 = ld_apex(M.geo, e1);
+            nl.x = p0.x * s + L1 * t;
+            nl.y = p0.y * s + 0.0 * t;
+            gpos = isect(last.x, last.y, cx, cy, L0, 0.0, ov.x, ov.y);
+            gpos = (1.0 - gpos) * L1;
+            gid = e1;
+            cx = L1 - gpos;
+        } else {
+            double2 p1 = ld_apex(M.geo, e2);
+            nl.x = 0.0 * s + p1.x * t;
+            nl.y = 0.0 * s + p1.y * t;
+            gpos = isect(last.x, last.y, cx, cy, ov.x, ov.y, 0.0, 0.0);
+            gpos = (1.0 - gpos) * L2;
+            gid = e2;
+            cx = L2 - gpos;
+        }
+        cy = 0.0;
+        last = nl;
+        src_edge = (uint32_t)gid;
+        src_x = gpos;
+        hg = ld_he(M.he, gid);
+        if (hg.twin < 0) { flags |= kFlagUndefined; return; }
+        opv = ld_he(M.he, nxt(hg.twin)).v1;
+    }
+}
+
+}  // namespace svgb

@@ -1,0 +1,427 @@
+// Batched shortest-path queries on the resident SVG (CSR).
+//
+// SVG::SolveSSSD / SolveMSAD (SVG.cu:241-251, 354-413) run a binary-heap A*
+// (Euclidean heuristic) or Dijkstra on the host, one query at a time.  Here
+// one thread block serves one query at a time, many blocks serve a batch,
+// and each query is a near-far label-correcting search:
+//   * a frontier ("near") of vertices whose distance improved and whose
+//     priority f = dist (+ |p - p_t| for SSSD) is below a threshold is
+//     relaxed in parallel, one warp per vertex, lanes over its edges;
+//     distances fall by 64-bit atomicMin on the double's bit pattern
+//     (non-negative doubles order like their bits), or, for MSAD with
+//     source ids, by a 16-byte compare-and-swap of {dist, src};
+//   * improved vertices above the threshold wait in a "far" list; when the
+//     near frontier drains, the threshold moves to the smallest waiting
+//     priority plus delta and those below it become the next frontier.
+// The result is the exact shortest-path distance (label correcting).  SSSD
+// stops once the target's distance is at most the threshold: with the
+// reference's consistent heuristic no unsettled path can then be shorter.
+// Per-slot stamp arrays replace clearing: a stamp is never reused.
+#include <cfloat>
+
+#include "engine.h"
+
+namespace svgb {
+
+namespace {
+
+constexpr int kQThreads = 512;
+constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;  // +inf
+
+struct alignas(16) DS {
+    unsigned long long d;  // double bits
+    long long s;           // source id (-1 = none)
+};
+
+struct QParams {
+    const int64_t* off;
+    const int32_t* adj;
+    const double* w;
+    const double* pos;     // 3*nv
+    int32_t nv;
+    int32_t n;             // queries
+    double delta;
+    // SSSD
+    const int32_t* s;
+    const int32_t* t;
+    double* out;           // n
+    // MSAD
+    const int64_t* set_off;
+    const int32_t* srcs;
+    const double* weights;
+    double* out_dist;      // n*nv
+    int32_t* out_src;      // n*nv or null
+    // scratch
+    char* scratch;
+    size_t slot_bytes;
+    uint32_t* slot_stamp;  // per slot
+    int32_t* head;
+    int64_t list_cap;      // far list capacity (entries)
+};
+
+__device__ __forceinline__ double hdist(const double* pos, int a, int b) {
+    double dx = pos[3 * a] - pos[3 * b], dy = pos[3 * a + 1] - pos[3 * b + 1], dz = pos[3 * a + 2] - pos[3 * b + 2];
+    return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+__device__ __forceinline__ double as_d(unsigned long long b) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ unsigned long long as_b(double d) { return (unsigned long long)__double_as_longlong(d); }
+
+struct Slot {
+    unsigned long long* dist;  // SSSD distances, nv, kept at +inf between queries
+    DS* ds;                    // MSAD {dist, src}, nv, initialised per query
+    uint32_t* nflag;           // nv
+    uint32_t* fflag;           // nv
+    int32_t* near;             // nv
+    int32_t* next;             // nv
+    int32_t* far;              // list_cap
+    int32_t* far2;             // list_cap
+    int32_t* touched;          // nv
+};
+
+__device__ Slot carve_slot(const QParams& P, int slot) {
+    char* p = P.scratch + (size_t)slot * P.slot_bytes;
+    size_t V = (size_t)P.nv;
+    auto take = [&](size_t bytes) { char* q = p; p += (bytes + 255) / 256 * 256; return q; };
+    Slot S;
+    S.dist = reinterpret_cast<unsigned long long*>(take(8 * V));
+    S.ds = reinterpret_cast<DS*>(take(16 * V));
+    S.nflag = reinterpret_cast<uint32_t*>(take(4 * V));
+    S.fflag = reinterpret_cast<uint32_t*>(take(4 * V));
+    S.near = reinterpret_cast<int32_t*>(take(4 * V));
+    S.next = reinterpret_cast<int32_t*>(take(4 * V));
+    S.far = reinterpret_cast<int32_t*>(take(4 * (size_t)P.list_cap));
+    S.far2 = reinterpret_cast<int32_t*>(take(4 * (size_t)P.list_cap));
+    S.touched = reinterpret_cast<int32_t*>(take(4 * V));
+    return S;
+}
+
+template <bool kSSSD, bool kSrc>
+__global__ void __launch_bounds__(kQThreads) k_query(QParams P) {
+    __shared__ int s_q;
+    __shared__ int s_nearN, s_nextN, s_farN, s_far2N, s_touchN;
+    __shared__ unsigned long long s_fmin;
+    __shared__ uint32_t s_stamp;
+    __shared__ int s_overflow;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = kQThreads / 32;
+    Slot S = carve_slot(P, blockIdx.x);
+    uint32_t* stamp_ctr = &P.slot_stamp[blockIdx.x];
+
+    for (;;) {
+        if (tid == 0) s_q = atomicAdd(P.head, 1);
+        __syncthreads();
+        const int q = s_q;
+        if (q >= P.n) break;
+        int tgt = -1;
+        if (kSSSD) tgt = P.t[q];
+        double thr;
+
+        // ---------------- initialise
+        if (tid == 0) {
+            s_nearN = 0; s_farN = 0; s_touchN = 0; s_overflow = 0;
+            s_stamp = *stamp_ctr + 1;
+        }
+        if (!kSSSD) {
+            for (int v = tid; v < P.nv; v += kQThreads) {
+                DS z;
+                z.d = kInfBits;
+                z.s = -1;
+                S.ds[v] = z;
+            }
+        }
+        __syncthreads();
+        const uint32_t fst = s_stamp;  // far-list stamp of the first phase
+        if (kSSSD) {
+            int s = P.s[q];
+            if (tid == 0) {
+                S.dist[s] = as_b(0.0);
+                S.touched[s_touchN++] = s;
+                S.far[s_farN++] = s;
+                S.fflag[s] = fst;
+            }
+        } else if (tid == 0) {
+            // SVG.cu:358-364: assignments in listed order, the last weight of a repeated source wins
+            int64_t b = P.set_off[q], e = P.set_off[q + 1];
+            for (int64_t i = b; i < e; ++i) {
+                DS z;
+                z.d = as_b(P.weights[i]);
+                z.s = P.srcs[i];
+                S.ds[P.srcs[i]] = z;
+            }
+            for (int64_t i = b; i < e; ++i) {
+                int v = P.srcs[i];
+                if (S.fflag[v] != fst) {
+                    S.fflag[v] = fst;
+                    S.far[s_farN++] = v;
+                }
+            }
+        }
+        __syncthreads();
+        thr = -1.0;
+        // every loop below is bounded: a query that needs more rounds than this
+        // reports -1 instead of spinning
+        const long long round_cap = 64LL * ((long long)P.nv + 16);
+        long long rounds = 0;
+
+        // ---------------- main loop: move the threshold, drain near frontiers
+        for (;;) {
+            if (++rounds > round_cap) {
+                if (tid == 0) s_overflow = 1;
+                __syncthreads();
+                break;
+            }
+            // smallest priority waiting in far
+            if (tid == 0) s_fmin = kInfBits;
+            __syncthreads();
+            const int farN = s_farN;
+            for (int i = tid; i < farN; i += kQThreads) {
+                int v = S.far[i];
+                double d = kSSSD ? as_d(S.dist[v]) : as_d(S.ds[v].d);
+                double f = kSSSD ? d + hdist(P.pos, v, tgt) : d;
+                atomicMin(&s_fmin, as_b(f));
+            }
+            __syncthreads();
+            if (farN == 0) break;
+            double fmin = as_d(s_fmin);
+            if (kSSSD) {
+                double dt = as_d(S.dist[tgt]);
+                if (dt <= fmin) break;  // no waiting path can beat the target's distance
+            }
+            thr = fmin + P.delta;
+            // split far: below the threshold -> near, the rest stays (deduplicated)
+            if (tid == 0) { s_nearN = 0; s_far2N = 0; s_stamp += 2; }
+            __syncthreads();
+            const uint32_t nst = s_stamp - 1, fst2 = s_stamp;
+            for (int i = tid; i < farN; i += kQThreads) {
+                int v = S.far[i];
+                double d = kSSSD ? as_d(S.dist[v]) : as_d(S.ds[v].d);
+                double f = kSSSD ? d + hdist(P.pos, v, tgt) : d;
+                if (f < thr) {
+                    if (atomicExch(&S.nflag[v], nst) != nst) S.near[atomicAdd(&s_nearN, 1)] = v;
+                } else if (atomicExch(&S.fflag[v], fst2) != fst2) {
+                    S.far2[atomicAdd(&s_far2N, 1)] = v;
+                }
+            }
+            __syncthreads();
+            {
+                int32_t* tmp = S.far; S.far = S.far2; S.far2 = tmp;
+            }
+            if (tid == 0) s_farN = s_far2N;
+            __syncthreads();
+
+            // drain the near frontier
+            while (s_nearN > 0) {
+                if (++rounds > round_cap) break;
+                const int nearN = s_nearN;
+                if (tid == 0) { s_nextN = 0; ++s_stamp; }
+                __syncthreads();
+                const uint32_t xst = s_stamp;
+                for (int i = warp; i < nearN; i += nwarps) {
+                    int u = S.near[i];
+                    double du;
+                    long long su = 0;
+                    if (kSSSD) {
+                        du = as_d(S.dist[u]);
+                    } else {
+                        DS z = S.ds[u];
+                        du = as_d(z.d);
+                        su = z.s;
+                    }
+                    int64_t e0 = P.off[u], e1 = P.off[u + 1];
+                    for (int64_t e = e0 + lane; e < e1; e += 32) {
+                        int w = P.adj[e];
+                        double nd = du + P.w[e];
+                        bool improved = false, first = false;
+                        if (kSSSD) {
+                            unsigned long long cur = S.dist[w];
+                            if (nd < as_d(cur)) {
+                                unsigned long long old = atomicMin(&S.dist[w], as_b(nd));
+                                improved = nd < as_d(old);
+                                first = old == kInfBits;
+                            }
+                        } else {
+                            DS cur = S.ds[w];
+                            while (nd < as_d(cur.d)) {
+                                DS nw;
+                                nw.d = as_b(nd);
+                                nw.s = su;
+                                DS prev = atomicCAS(&S.ds[w], cur, nw);
+                                if (prev.d == cur.d && prev.s == cur.s) { improved = true; break; }
+                                cur = prev;
+                            }
+                        }
+                        if (!improved) continue;
+                        if (kSSSD && first) {
+                            int k = atomicAdd(&s_touchN, 1);
+                            S.touched[k] = w;
+                        }
+                        double f = kSSSD ? nd + hdist(P.pos, w, tgt) : nd;
+                        if (f < thr) {
+                            if (atomicExch(&S.nflag[w], xst) != xst) S.next[atomicAdd(&s_nextN, 1)] = w;
+                        } else if (atomicExch(&S.fflag[w], fst2) != fst2) {
+                            int k = atomicAdd(&s_farN, 1);
+                            if (k < P.list_cap) S.far[k] = w;
+                            else s_overflow = 1;
+                        }
+                    }
+                }
+                __syncthreads();
+                {
+                    int32_t* tmp = S.near; S.near = S.next; S.next = tmp;
+                }
+                if (tid == 0) s_nearN = s_nextN;
+                __syncthreads();
+            }
+            if (rounds > round_cap && tid == 0) s_overflow = 1;
+            __syncthreads();
+            if (s_overflow) break;
+        }
+        __syncthreads();
+
+        // ---------------- results
+        if (kSSSD) {
+            if (tid == 0) {
+                unsigned long long dt = S.dist[tgt];
+                P.out[q] = s_overflow ? -1.0 : (dt == kInfBits ? DBL_MAX : as_d(dt));
+            }
+            __syncthreads();
+            const int tn = s_touchN;
+            for (int i = tid; i < tn; i += kQThreads) S.dist[S.touched[i]] = kInfBits;
+        } else {
+            double* od = P.out_dist + (size_t)q * P.nv;
+            int32_t* os = kSrc ? P.out_src + (size_t)q * P.nv : nullptr;
+            for (int v = tid; v < P.nv; v += kQThreads) {
+                DS z = S.ds[v];
+                od[v] = z.d == kInfBits ? DBL_MAX : (s_overflow ? -1.0 : as_d(z.d));
+                if (kSrc) os[v] = (int32_t)z.s;
+            }
+        }
+        if (tid == 0) *stamp_ctr = s_stamp;
+        __syncthreads();
+    }
+}
+
+__global__ void k_mean_weight(const double* w, int64_t n, double* out) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += w[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, s[0]);
+}
+
+__global__ void k_fill(unsigned long long* p, size_t n, unsigned long long v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+struct QState {
+    double delta = 0.0;
+    int slots = 0;          // slots initialised in g->qbuf
+    size_t slot_bytes = 0;
+};
+
+QState& qstate(svg_graph* g) {
+    static std::vector<std::pair<svg_graph*, QState>> tab;
+    for (auto& p : tab)
+        if (p.first == g) return p.second;
+    tab.emplace_back(g, QState{});
+    return tab.back().second;
+}
+
+size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Prepare per-block scratch for up to `want` concurrent query slots; returns
+// the slot count (= grid size).
+int prepare(svg_graph* g, int want, QParams& P) {
+    cudaStream_t st = lib_stream();
+    QState& Q = qstate(g);
+    if (Q.delta == 0.0) {
+        double* d_sum = nullptr;
+        SVG_CUDA(cudaMalloc(&d_sum, sizeof(double)));
+        SVG_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), st));
+        if (g->nnz > 0) k_mean_weight<<<256, 256, 0, st>>>(g->dist, g->nnz, d_sum);
+        double sum = 0.0;
+        SVG_CUDA(cudaMemcpyAsync(&sum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, st));
+        SVG_CUDA(cudaStreamSynchronize(st));
+        cudaFree(d_sum);
+        double mean = g->nnz > 0 ? sum / (double)g->nnz : 1.0;
+        Q.delta = mean > 0.0 ? mean : 1.0;
+    }
+    int dev = 0;
+    SVG_CUDA(cudaGetDevice(&dev));
+    int sms = 0;
+    SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int slots = std::max(1, std::min(want, sms * 2));
+    size_t V = (size_t)g->nv;
+    int64_t list_cap = 2 * (int64_t)V + 64;
+    size_t slot_bytes = al256(8 * V) + al256(16 * V) + 4 * al256(4 * V) + 2 * al256(4 * (size_t)list_cap) + al256(4 * V);
+    if (Q.slots < slots || Q.slot_bytes != slot_bytes) {
+        int ns = std::max(slots, Q.slots);
+        size_t need = al256((size_t)ns * slot_bytes) + al256(sizeof(uint32_t) * (size_t)ns) + 256;
+        g->qbuf.reserve(need);
+        SVG_CUDA(cudaMemsetAsync(g->qbuf.p, 0, need, st));  // stamps and flags start at 0
+        for (int sl = 0; sl < ns; ++sl)  // SSSD distances start at +inf
+            k_fill<<<64, 256, 0, st>>>(reinterpret_cast<unsigned long long*>(g->qbuf.as<char>() + (size_t)sl * slot_bytes),
+                                      V, kInfBits);
+        SVG_CUDA(cudaGetLastError());
+        Q.slots = ns;
+        Q.slot_bytes = slot_bytes;
+    }
+    char* base = g->qbuf.as<char>();
+    P.scratch = base;
+    P.slot_bytes = slot_bytes;
+    P.slot_stamp = reinterpret_cast<uint32_t*>(base + al256((size_t)Q.slots * slot_bytes));
+    P.head = reinterpret_cast<int32_t*>(base + al256((size_t)Q.slots * slot_bytes) + al256(sizeof(uint32_t) * (size_t)Q.slots));
+    P.list_cap = list_cap;
+    P.off = g->off;
+    P.adj = g->adj;
+    P.w = g->dist;
+    P.pos = g->mesh->d.pos;
+    P.nv = g->nv;
+    P.delta = Q.delta;
+    SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
+    return slots;
+}
+
+}  // namespace
+
+svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist) {
+    if (n == 0) return SVG_OK;
+    QParams P{};
+    int slots = prepare(g, n, P);
+    P.n = n;
+    P.s = d_s;
+    P.t = d_t;
+    P.out = d_dist;
+    k_query<true, false><<<slots, kQThreads, 0, lib_stream()>>>(P);
+    SVG_CUDA(cudaGetLastError());
+    return SVG_OK;
+}
+
+svg_status run_msad(svg_graph* g, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w,
+                    double* d_dist, int32_t* d_src_id, int64_t total_srcs) {
+    (void)total_srcs;
+    if (n == 0) return SVG_OK;
+    QParams P{};
+    int slots = prepare(g, n, P);
+    P.n = n;
+    P.set_off = d_off;
+    P.srcs = d_src;
+    P.weights = d_w;
+    P.out_dist = d_dist;
+    P.out_src = d_src_id;
+    if (d_src_id)
+        k_query<false, true><<<slots, kQThreads, 0, lib_stream()>>>(P);
+    else
+        k_query<false, false><<<slots, kQThreads, 0, lib_stream()>>>(P);
+    SVG_CUDA(cudaGetLastError());
+    return SVG_OK;
+}
+
+}  // namespace svgb

@@ -1,0 +1,132 @@
+"""Parity of the CUDA SVG construction with the reference (GPU).
+
+Bit-exact: neighbour sets, edge lengths and path-end fields of every row
+must equal the reference's (golden fixtures) or the oracle's (the C
+restatement pinned to the reference) on the same inputs.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle.refbind import CpuOracle
+from svg_b200 import MODE_BATCHED, MODE_PLAIN, SVG, Mesh, meshgen
+from svg_b200.build_ext import build as build_lib
+from tests.helpers import compare_rows, golden_params, load_golden, rows_from_padded, svg_file_bytes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    build_lib()
+
+
+def gpu_build(pos, faces, K, mode=MODE_BATCHED, **kw):
+    m = Mesh.from_arrays(pos, faces)
+    s = SVG()
+    s.AssignMesh(m)
+    s.SetParameters(K, kw.pop("split_coef", 10), kw.pop("vert_coef", 2))
+    st = s.ConstructSVG(mode=mode, **kw)
+    off, nodes = s.CopySVGToHost()
+    return off, nodes, st, s, m
+
+
+@pytest.mark.parametrize("mode", [MODE_BATCHED, MODE_PLAIN])
+@pytest.mark.parametrize("name,K", golden_params())
+def test_build_matches_reference_golden(name, K, mode):
+    g = load_golden(name)
+    off, nodes, st, _, _ = gpu_build(g["pos"], g["faces"], K, mode)
+    goff, gnodes = rows_from_padded(g[f"K{K}_tails"], g[f"K{K}_nodes"])
+    assert compare_rows(off, nodes, goff, gnodes) == []
+    assert st["windows_generated"] == int(g[f"K{K}_stats"][:, 0].sum())
+    assert st["watchdog_sources"] == 0
+
+
+def _oracle_rows(pos, faces, K, src, **kw):
+    rows = CpuOracle().mesh(pos, faces).build(K, src, threads=0, **kw)
+    return rows_from_padded(rows.tails, rows.nodes), rows
+
+
+@pytest.mark.parametrize("cfg,K,ranges", [
+    (0, 100, [(0, 768), (15000, 15512)]),
+    (1, 500, [(0, 300), (36300, 36556)]),
+    (1, 100, [(72500, 72900)]),
+])
+def test_build_matches_oracle_on_benchmark_mesh_samples(cfg, K, ranges):
+    pos, faces = meshgen.config_mesh(cfg)
+    for a, b in ranges:
+        off, nodes, st, _, m = gpu_build(pos, faces, K, source_begin=a, source_end=b)
+        src = np.arange(a, b, dtype=np.int32)
+        (ooff, onodes), rows = _oracle_rows(pos, faces, K, src)
+        sub = off[a:b + 1] - off[a]
+        got = nodes[off[a]:off[b]]
+        assert compare_rows(sub, got, ooff, onodes) == []
+        assert st["windows_generated"] == int(rows.stats[:, 0].sum())
+        assert off[b] - off[a] == off[-1]  # rows outside the range are empty
+
+
+def test_queue_capacity_drops_like_the_reference():
+    pos, faces = meshgen.torus(1.0, 0.35, 24, 16, 0.02, seed=3)
+    for mode in (MODE_BATCHED, MODE_PLAIN):
+        off, nodes, st, _, _ = gpu_build(pos, faces, 30, mode, win_queue_cap=12, pseudo_queue_cap=5)
+        (ooff, onodes), rows = _oracle_rows(pos, faces, 30, None, win_cap=12, pseudo_cap=5)
+        assert compare_rows(off, nodes, ooff, onodes) == []
+        assert st["queue_drop_sources"] > 0
+
+
+def test_plain_and_batched_builds_are_identical():
+    pos, faces = meshgen.height_field(40, seed=7)
+    a = gpu_build(pos, faces, 60, MODE_BATCHED)
+    b = gpu_build(pos, faces, 60, MODE_PLAIN)
+    assert compare_rows(a[0], a[1], b[0], b[1]) == []
+    assert a[2]["windows"] == b[2]["windows"]
+
+
+def test_csr_without_paths_matches():
+    pos, faces = meshgen.torus(1.0, 0.35, 30, 20, 0.02, seed=5)
+    off, nodes, _, s, _ = gpu_build(pos, faces, 40, with_paths=False)
+    coff, adj, dist = s.csr()
+    (ooff, onodes), _ = _oracle_rows(pos, faces, 40, None)
+    assert np.array_equal(coff, ooff)
+    assert np.array_equal(adj, onodes["adj"])
+    assert np.array_equal(dist, onodes["dist"])
+
+
+def test_save_file_is_byte_identical_to_reference_format():
+    g = load_golden("monkey")
+    K = 20
+    _, _, _, s, m = gpu_build(g["pos"], g["faces"], K)
+    goff, gnodes = rows_from_padded(g[f"K{K}_tails"], g[f"K{K}_nodes"])
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "m.svg")
+        s.SaveSVGToFile(p)
+        data = open(p, "rb").read()
+        gn = gnodes.copy()
+        gn["pad"] = 0
+        assert data == svg_file_bytes(goff, gn)
+        s2 = SVG()
+        s2.AssignMesh(m)
+        s2.SetParameters(K)
+        s2.LoadSVGFromFile(p)
+        off2, n2 = s2.CopySVGToHost()
+        assert compare_rows(off2, n2, goff, gnodes) == []
+
+
+def test_per_source_statistics():
+    pos, faces = meshgen.torus(1.0, 0.35, 30, 20, 0.02, seed=5)
+    _, _, st, s, _ = gpu_build(pos, faces, 40)
+    w, q, f = s.source_stats()
+    assert w.sum() == st["windows"]
+    assert q.max() == st["max_win_queue"]
+    assert (f == 0).all()
+
+
+def test_bad_arguments_are_reported():
+    from svg_b200 import SvgError
+    pos, faces = meshgen.torus(1.0, 0.35, 8, 6, 0.02, seed=5)
+    with pytest.raises(SvgError):
+        gpu_build(pos, faces, 0)
+    with pytest.raises(SvgError):
+        gpu_build(pos, faces, 10, source_begin=10, source_end=5)

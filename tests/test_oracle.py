@@ -1,0 +1,120 @@
+"""The C restatement (oracle/svg_oracle.c) pinned against the reference.
+
+Two pins: the committed golden fixtures (tests/golden, produced by running the
+reference's own ICH), and - where the reference sources are checked out - the
+reference oracle itself (oracle/_ref) on samples of the benchmark meshes.
+Both must agree bit for bit, every node field.
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle.refbind import CpuOracle, RefOracle, ref_available, rows_equal, REF_LIB, HERE as ORACLE_DIR
+from svg_b200 import meshgen
+from tests.helpers import golden_params, load_golden, rows_from_padded, compare_rows
+
+REF_SRC = os.environ.get("SVG_REFERENCE_DIR", "/root/reference")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not ref_available() and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "ref", "REF=" + REF_SRC], check=True)
+    if not ref_available():
+        pytest.skip("reference oracle not built (reference sources absent)")
+    return RefOracle()
+
+
+@pytest.mark.parametrize("name,K", golden_params())
+def test_restatement_matches_golden(name, K):
+    g = load_golden(name)
+    m = CpuOracle().mesh(g["pos"], g["faces"])
+    ex = m.export()
+    assert np.array_equal(ex["he_twin"], g["he_twin"])
+    assert np.array_equal(ex["he_len"], g["he_len"])
+    assert np.array_equal(ex["angle"], g["angle"])
+    assert np.array_equal(ex["first_edge"], g["first_edge"])
+    rows = m.build(K, threads=2)
+    offa, na = rows_from_padded(rows.tails, rows.nodes)
+    offb, nb = rows_from_padded(g[f"K{K}_tails"], g[f"K{K}_nodes"])
+    assert compare_rows(offa, na, offb, nb) == []
+    # the reference's ICH counters: windows generated, vertices counted
+    assert np.array_equal(rows.stats[:, 0], g[f"K{K}_stats"][:, 0])
+    assert np.array_equal(rows.stats[:, 3], g[f"K{K}_stats"][:, 3])
+
+
+@pytest.mark.parametrize("cfg,K,n", [(0, 100, 48), (1, 500, 24), (1, 100, 48)])
+def test_restatement_matches_reference_on_benchmark_meshes(ref, cfg, K, n):
+    pos, faces = meshgen.config_mesh(cfg)
+    with tempfile.TemporaryDirectory() as td:
+        obj = os.path.join(td, "m.obj")
+        meshgen.write_obj(obj, pos, faces)
+        rm = ref.load(obj, fix_boundary=True)
+        cm = CpuOracle().mesh(pos, faces)
+        src = np.random.default_rng(11 + cfg).choice(rm.nv, n, replace=False).astype(np.int32)
+        a = rm.build(K, src, threads=0)
+        b = cm.build(K, src, threads=0)
+        ok, msg = rows_equal(a, b)
+        assert ok, msg
+        assert np.array_equal(a.stats[:, [0, 3]], b.stats[:, [0, 3]])
+
+
+def test_restatement_queue_cap_and_small_tables_match_reference(ref):
+    """Small queues drop pushes (PriorityQueue.cuh:53); the restatement drops
+    the same windows as the reference."""
+    pos, faces = meshgen.torus(1.0, 0.35, 24, 16, 0.02, seed=3)
+    with tempfile.TemporaryDirectory() as td:
+        obj = os.path.join(td, "m.obj")
+        meshgen.write_obj(obj, pos, faces)
+        rm = ref.load(obj)
+        cm = CpuOracle().mesh(pos, faces)
+        # (tables small enough to overflow make the reference itself spin: not compared)
+        for K, sc, vc, wc, pc in [(30, 10, 2, 12, 5), (40, 4, 2, 40, 8), (60, 10, 2, 30, 1023)]:
+            a = rm.build(K, None, threads=0, split_coef=sc, vert_coef=vc, win_cap=wc, pseudo_cap=pc)
+            b = cm.build(K, None, threads=0, split_coef=sc, vert_coef=vc, win_cap=wc, pseudo_cap=pc)
+            ok, msg = rows_equal(a, b)
+            assert ok, (K, sc, vc, wc, pc, msg)
+
+
+def test_query_restatement_matches_reference(ref):
+    g = load_golden("torus_small")
+    K = 30
+    tails, nodes = g[f"K{K}_tails"], g[f"K{K}_nodes"]
+    with tempfile.TemporaryDirectory() as td:
+        obj = os.path.join(td, "m.obj")
+        meshgen.write_obj(obj, g["pos"], g["faces"])
+        rm = ref.load(obj)
+        cm = CpuOracle().mesh(g["pos"], g["faces"])
+        off, packed = rows_from_padded(tails, nodes)
+        rng = np.random.default_rng(2)
+        s = rng.integers(0, rm.nv, 40).astype(np.int32)
+        t = rng.integers(0, rm.nv, 40).astype(np.int32)
+        d_ref, _ = rm.sssd(K, tails, nodes, s, t)
+        d_cpu, _ = cm.sssd(off, packed["adj"], packed["dist"], s, t)
+        assert np.array_equal(d_ref, d_cpu)
+        srcs = rng.choice(rm.nv, 5, replace=False).astype(np.int32)
+        w = rng.uniform(0, 0.2, 5)
+        dr, sr, _ = rm.msad(K, tails, nodes, srcs, w)
+        dc, sc, _ = cm.msad(off, packed["adj"], packed["dist"], srcs, w)
+        assert np.array_equal(dr, dc)
+        assert np.array_equal(sr, sc)
+
+
+def test_exact_ich_restatement_matches_reference(ref):
+    """Exhaustive ICH (K = -1), the accuracy oracle, agrees with the reference."""
+    pos, faces = meshgen.height_field(14, seed=1)
+    with tempfile.TemporaryDirectory() as td:
+        obj = os.path.join(td, "m.obj")
+        meshgen.write_obj(obj, pos, faces)
+        rm = ref.load(obj)
+        cm = CpuOracle().mesh(pos, faces)
+        src = np.array([0, 7, 100, 195], np.int32)
+        da, _, _ = rm.ich_distances(src, K=-1, win_cap=1 << 16, pseudo_cap=1 << 14)
+        db, _, _ = cm.ich_distances(src, K=-1, win_cap=1 << 16, pseudo_cap=1 << 14)
+        assert np.array_equal(da, db)
+        # from an interior source the exhaustive ICH reaches every vertex (from a
+        # boundary corner the reference's Initialize covers part of the fan only)
+        assert np.all(da[2] < np.finfo(np.float64).max)

@@ -1,0 +1,89 @@
+"""Batched SSSD / MSAD queries on the device vs the reference's host A* and
+Dijkstra (restated in the oracle), within 1e-8 relative distance."""
+import numpy as np
+import pytest
+
+from oracle.refbind import CpuOracle
+from svg_b200 import SVG, Mesh, meshgen
+from svg_b200.build_ext import build as build_lib
+
+pytestmark = pytest.mark.gpu
+DBL_MAX = np.finfo(np.float64).max
+RTOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def graph():
+    build_lib()
+    pos, faces = meshgen.torus(1.0, 0.35, 60, 40, 0.02, seed=9)
+    m = Mesh.from_arrays(pos, faces)
+    s = SVG()
+    s.AssignMesh(m)
+    s.SetParameters(50)
+    s.ConstructSVG()
+    off, adj, dist = s.csr()
+    cm = CpuOracle().mesh(pos, faces)
+    return s, m, cm, off, adj, dist
+
+
+def rel_err(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+def test_sssd_batch_matches_reference_astar(graph):
+    s, m, cm, off, adj, dist = graph
+    rng = np.random.default_rng(1)
+    S = rng.integers(0, m.vertNum, 300).astype(np.int32)
+    T = rng.integers(0, m.vertNum, 300).astype(np.int32)
+    got = s.sssd_batch(S, T)
+    ref, _ = cm.sssd(off, adj, dist, S, T)
+    assert np.all(rel_err(got, ref) <= RTOL)
+
+
+def test_sssd_same_vertex_and_single_query(graph):
+    s, m, cm, off, adj, dist = graph
+    assert s.SolveSSSD(5, 5) == 0.0
+    ref, _ = cm.sssd(off, adj, dist, [3], [700])
+    assert rel_err(np.array([s.SolveSSSD(3, 700)]), ref)[0] <= RTOL
+
+
+def test_msad_batch_matches_reference_dijkstra(graph):
+    s, m, cm, off, adj, dist = graph
+    rng = np.random.default_rng(2)
+    sets = [rng.choice(m.vertNum, k, replace=False).astype(np.int32) for k in (1, 3, 17, 200)]
+    weights = [rng.uniform(0, 0.3, len(x)) for x in sets]
+    d, src = s.msad_batch(sets, weights)
+    for q in range(len(sets)):
+        rd, rs, _ = cm.msad(off, adj, dist, sets[q], weights[q])
+        assert np.all(rel_err(d[q], rd) <= RTOL)
+        # source ids agree wherever the winning source is unambiguous
+        assert (src[q] == rs).mean() > 0.999
+
+
+def test_msad_repeated_source_keeps_last_weight(graph):
+    s, m, cm, off, adj, dist = graph
+    srcs = np.array([10, 400, 10], np.int32)
+    w = np.array([0.0, 0.05, 0.5])
+    d, _ = s.SolveMSAD(srcs, w)
+    rd, _, _ = cm.msad(off, adj, dist, srcs, w)
+    assert d[10] == 0.5
+    assert np.all(rel_err(d, rd) <= RTOL)
+
+
+def test_unreachable_vertices_report_dbl_max():
+    build_lib()
+    a, fa = meshgen.torus(1.0, 0.3, 10, 8, 0.0, seed=1)
+    b, fb = meshgen.torus(1.0, 0.3, 10, 8, 0.0, seed=1)
+    b = b + np.array([5.0, 0.0, 0.0])
+    pos = np.vstack([a, b])
+    faces = np.vstack([fa, fb + len(a)])
+    m = Mesh.from_arrays(pos, faces)
+    s = SVG()
+    s.AssignMesh(m)
+    s.SetParameters(20)
+    s.ConstructSVG()
+    assert s.SolveSSSD(0, len(a) + 3) == DBL_MAX
+    d, src = s.SolveMSAD([1], [0.0])
+    assert np.all(d[len(a):] == DBL_MAX)
+    assert np.all(src[len(a):] == -1)
+    assert np.all(d[:len(a)] < DBL_MAX)
