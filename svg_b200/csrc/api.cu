@@ -44,6 +44,9 @@ void DevBuf::release() {
 
 DevMesh MeshDev::view() const {
     DevMesh v{};
+    v.nv = nv;
+    v.nf = nf;
+    v.ne = ne;
     v.he = he;
     v.geo = geo;
     v.vr = vr;
@@ -65,6 +68,9 @@ void upload_mesh(svg_mesh* m) {
     SVG_CUDA(cudaMemcpyAsync(D.vr, H.vr.data(), sizeof(VertRec) * (size_t)H.nv, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.pos, H.pos.data(), sizeof(double) * 3 * (size_t)H.nv, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaStreamSynchronize(st));
+    D.nv = H.nv;
+    D.nf = H.nf;
+    D.ne = H.ne;
     D.uploaded = true;
 }
 

@@ -45,6 +45,7 @@ struct DevBuf {
 
 struct MeshDev {
     bool uploaded = false;
+    int32_t nv = 0, nf = 0, ne = 0;
     HeRec* he = nullptr;
     HeGeo* geo = nullptr;
     VertRec* vr = nullptr;
