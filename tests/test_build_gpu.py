@@ -36,12 +36,29 @@ def gpu_build(pos, faces, K, mode=MODE_BATCHED, **kw):
 @pytest.mark.parametrize("mode", [MODE_BATCHED, MODE_PLAIN])
 @pytest.mark.parametrize("name,K", golden_params())
 def test_build_matches_reference_golden(name, K, mode):
+    """Rows bit-exact against the reference.  Where the reference's fixed
+    vertex/split hash tables (K*2, K*10 slots) overflow into their shared sink
+    slot, the reference's search is no longer an ICH; such sources must be
+    flagged (bit 2) and are excluded, their counters too."""
     g = load_golden(name)
-    off, nodes, st, _, _ = gpu_build(g["pos"], g["faces"], K, mode)
+    off, nodes, st, s, _ = gpu_build(g["pos"], g["faces"], K, mode)
+    _, _, flags = s.source_stats()
     goff, gnodes = rows_from_padded(g[f"K{K}_tails"], g[f"K{K}_nodes"])
-    assert compare_rows(off, nodes, goff, gnodes) == []
-    assert st["windows_generated"] == int(g[f"K{K}_stats"][:, 0].sum())
+    ok_rows = [r for r in range(len(off) - 1) if not (flags[r] & 2)]
+    assert compare_rows(off, nodes, goff, gnodes, rows=ok_rows) == []
+    if st["ref_overflow_sources"] == 0:
+        assert st["windows_generated"] == int(g[f"K{K}_stats"][:, 0].sum())
     assert st["watchdog_sources"] == 0
+
+
+def test_reference_table_overflow_is_flagged():
+    """monkey, K=6: the centre reaches 13 vertices, the reference's vertex
+    table holds 2K = 12 keys."""
+    g = load_golden("monkey")
+    _, _, st, s, _ = gpu_build(g["pos"], g["faces"], 6)
+    _, _, flags = s.source_stats()
+    assert flags[0] & 2
+    assert st["ref_overflow_sources"] >= 1
 
 
 def _oracle_rows(pos, faces, K, src, **kw):
