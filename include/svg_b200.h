@@ -180,6 +180,30 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
                                  const int32_t* d_srcs, const double* d_weights, double* d_dist,
                                  int32_t* d_src_id);
 
+/* Allocation-free build of SVG rows.  No counterpart in the reference (its
+ * SVG::Allocation cudaMallocs every buffer); it is for callers that cannot
+ * allocate device memory at this point - code whose allocations all belong
+ * to an outer framework's pool, or that runs where a cudaMalloc would
+ * synchronise the device or break a capture.  The caller provides every
+ * buffer; the kernel's scratch is a fixed array inside the library (about
+ * 15 MiB per GPU that loads the library, held until the library unloads).
+ *   m            a mesh already on the device (svg_mesh_upload, which does
+ *                allocate, must have been called earlier)
+ *   K            1..128 (queue capacities are the reference's 1023)
+ *   [source_begin, source_end)  sources to build, row r = source_begin + r
+ *   d_tails      device int32[n]: row length, or -1 if that source outgrew
+ *                the fixed tables
+ *   d_adj, d_dist  device int32[n*K], double[n*K]: padded rows, the same
+ *                neighbours and lengths as svg_build's rows
+ *   stream       cudaStream_t (NULL: the legacy default stream)
+ * Asynchronous: outputs are complete when the stream reaches this point.
+ * All calls share the one scratch array, so calls whose kernels could run
+ * at the same time on the GPU race; serialise them.  The first call on each
+ * device looks up the array's device address; make that first call before
+ * any stream capture. */
+svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t source_begin, int32_t source_end,
+                                 int32_t* d_tails, int32_t* d_adj, double* d_dist, void* stream);
+
 /* Synchronise the library's stream; returns the device time in ms since the
  * previous svg_timer_mark (CUDA events on the library stream). */
 svg_status svg_timer_mark(double* ms_since_last);

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "engine.h"
 #include "ich.cuh"
@@ -757,3 +758,168 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
 }
 
 }  // namespace svgb
+
+// ---------------------------------------------------------------------------
+// Allocation-free build entry point (svg_build_rows_static).
+//
+// For callers that must not allocate device memory themselves or through the
+// library - e.g. code running inside a framework that owns every allocation
+// through its own pool, or a process that captures work into a graph whose
+// memory must not change - this variant of the plain build keeps all of its
+// lane scratch in one fixed array linked into the library, and writes into
+// output buffers the caller provides.
+//
+// Limits: kStaticLanes = 128 lanes (one source each at a time, grid-stride
+// over the range), K <= kStaticMaxK = 128, queue capacities fixed at the
+// reference's 1023, tables sized for K = 128.  The array takes
+// kStaticScratchBytes (about 15 MiB) on every GPU that loads the library, for
+// as long as the library stays loaded.  All calls share it: two calls whose
+// kernels overlap on the GPU (different streams, or different host threads)
+// race on it and produce garbage; serialise them.  Each source resets its own
+// tables before it starts, so nothing carried over from an earlier call is
+// ever read and the array never needs clearing.
+// ---------------------------------------------------------------------------
+namespace svgb {
+namespace {
+
+constexpr int kStaticLanes = 128;
+constexpr int kStaticMaxK = 128;
+constexpr int kStaticWcap = 1023;
+constexpr int kStaticPcap = 1023;
+constexpr int kStaticVcapLog2 = 9;  // 512 slots >= 2 * (2*128 + 1)
+constexpr int kStaticScapLog2 = 9;  // 512 slots >= 4 * 128
+constexpr int kStaticVlimit = 384;
+constexpr int kStaticSlimit = 384;
+
+constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t kSzWheap = al256((size_t)kStaticLanes * (kStaticWcap + 1) * sizeof(WinEntry));
+constexpr size_t kSzWpool = al256((size_t)kStaticLanes * kStaticWcap * sizeof(WinPay));
+constexpr size_t kSzWfree = al256((size_t)kStaticLanes * kStaticWcap * sizeof(uint16_t));
+constexpr size_t kSzPheap = al256((size_t)kStaticLanes * (kStaticPcap + 1) * sizeof(PsEntry));
+constexpr size_t kSzVtab = al256((size_t)kStaticLanes * ((size_t)1 << kStaticVcapLog2) * sizeof(VSlot));
+constexpr size_t kSzVlist = al256((size_t)kStaticLanes * kStaticVlimit * sizeof(int32_t));
+constexpr size_t kSzStab = al256((size_t)kStaticLanes * ((size_t)1 << kStaticScapLog2) * sizeof(SSlot));
+constexpr size_t kSzEpoch = al256((size_t)kStaticLanes * sizeof(uint32_t));
+constexpr size_t kStaticScratchBytes =
+    kSzWheap + kSzWpool + kSzWfree + kSzPheap + kSzVtab + kSzVlist + kSzStab + kSzEpoch;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch, resolved once per device.  In host code
+// the array's name is only a host-side stand-in for the symbol, never a
+// device address.
+constexpr int kMaxDevices = 64;
+void* g_static_ptr[kMaxDevices] = {nullptr};
+std::mutex g_static_mu;
+
+void* static_scratch_address() {
+    int dev = 0;
+    SVG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw SvgError{SVG_ERR_ARG, "device ordinal out of range"};
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            throw SvgError{SVG_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch) failed: ") +
+                                             cudaGetErrorString(e)};
+        }
+        g_static_ptr[dev] = p;
+    }
+    return g_static_ptr[dev];
+}
+
+struct StaticOut {
+    int32_t source_begin;
+    int32_t nsrc;
+    int32_t* tails;
+    int32_t* adj;
+    double* dist;
+};
+
+// The plain build (k_ich_plain) with its scratch carved from the static array.
+__global__ void __launch_bounds__(128) k_ich_static(LaneConfig C, StaticOut O) {
+    int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    int stride = gridDim.x * blockDim.x;
+    Lane L(C, gtid);
+    const int K = C.K;
+    for (int r = gtid; r < O.nsrc; r += stride) {
+        int v = O.source_begin + r;
+        L.begin(v, true);
+        while (!L.step()) {
+        }
+        int tail = 0;
+        size_t row = (size_t)r * K;
+        if (L.flags & kFlagCapacity) {
+            O.tails[r] = -1;  // the source outgrew the static tables
+            continue;
+        }
+        for (int j = 0; j < C.M.nv && K > 0; ++j) {
+            double d = L.vdist(j);
+            if (d == DBL_MAX || j == v) continue;
+            uint32_t se, de;
+            double sx = 0.0, dx = 0.0;
+            if (trace_full(L, j, se, sx, de, dx)) continue;
+            O.adj[row + tail] = j;
+            O.dist[row + tail] = d;
+            if (++tail == K) break;
+        }
+        O.tails[r] = tail;
+    }
+}
+
+}  // namespace
+}  // namespace svgb
+
+extern "C" svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t source_begin, int32_t source_end,
+                                            int32_t* d_tails, int32_t* d_adj, double* d_dist, void* stream) {
+    using namespace svgb;
+    try {
+        set_error("");
+        if (!m || !d_tails || !d_adj || !d_dist) throw SvgError{SVG_ERR_ARG, "null argument"};
+        if (!m->d.uploaded)
+            throw SvgError{SVG_ERR_STATE, "mesh not on the device: call svg_mesh_upload first (it allocates)"};
+        if (K < 1 || K > kStaticMaxK)
+            throw SvgError{SVG_ERR_ARG, "K = " + std::to_string(K) + " outside [1, " + std::to_string(kStaticMaxK) +
+                                            "], the limit of the allocation-free build"};
+        if (source_begin < 0 || source_end > m->h.nv || source_begin > source_end)
+            throw SvgError{SVG_ERR_ARG, "source range outside [0, nv]"};
+        const int32_t nsrc = source_end - source_begin;
+        if (nsrc == 0) return SVG_OK;
+        char* base = static_cast<char*>(static_scratch_address());
+        LaneConfig C{};
+        C.M = m->d.view();
+        C.K = K;
+        C.wcap = kStaticWcap;
+        C.pcap = kStaticPcap;
+        C.vref = (uint32_t)K * 2;
+        C.sref = (uint32_t)K * 10;
+        C.vcap_log2 = kStaticVcapLog2;
+        C.scap_log2 = kStaticScapLog2;
+        C.vlimit = kStaticVlimit;
+        C.slimit = kStaticSlimit;
+        C.watchdog = (int64_t)1 << 26;
+        char* p = base;
+        C.wheap = reinterpret_cast<WinEntry*>(p); p += kSzWheap;
+        C.wpool = reinterpret_cast<WinPay*>(p); p += kSzWpool;
+        C.wfree = reinterpret_cast<uint16_t*>(p); p += kSzWfree;
+        C.pheap = reinterpret_cast<PsEntry*>(p); p += kSzPheap;
+        C.vtab = reinterpret_cast<VSlot*>(p); p += kSzVtab;
+        C.vlist = reinterpret_cast<int32_t*>(p); p += kSzVlist;
+        C.stab = reinterpret_cast<SSlot*>(p); p += kSzStab;
+        C.epochs = reinterpret_cast<uint32_t*>(p);
+        StaticOut O{source_begin, nsrc, d_tails, d_adj, d_dist};
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        k_ich_static<<<kStaticLanes / 128, 128, 0, st>>>(C, O);
+        SVG_CUDA(cudaGetLastError());
+        return SVG_OK;
+    } catch (const SvgError& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const CudaFail& e) {
+        cudaGetLastError();
+        set_error(std::string("CUDA error ") + cudaGetErrorString(e.err) + " in " + e.where);
+        return SVG_ERR_CUDA;
+    }
+}
