@@ -27,7 +27,7 @@ __all__ = ["Mesh", "SVG", "BuildOptions", "SvgError", "lib", "NODE_DTYPE", "LIB_
            "MODE_BATCHED", "MODE_PLAIN"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsvg_b200.so")
+LIB_PATH = os.environ.get("SVG_B200_LIB") or os.path.join(HERE, "libsvg_b200.so")
 MODE_BATCHED, MODE_PLAIN = 0, 1
 DBL_MAX = np.finfo(np.float64).max
 

@@ -50,19 +50,21 @@ def _run(cmd, log):
     return r.stdout + r.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OUT_DIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, out_dir: str = OUT_DIR, lib: str = LIB,
+          defines: tuple = ()) -> str:
+    """Compile (incrementally) into `lib`; `defines` are extra -D flags for the CUDA sources."""
+    os.makedirs(out_dir, exist_ok=True)
     jobs = []
     objs = []
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(OUT_DIR, s + ".o")
+        obj = os.path.join(out_dir, s + ".o")
         objs.append(obj)
         if force or _stale(obj, src):
-            jobs.append(([NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj], obj + ".log"))
+            jobs.append(([NVCC] + NVCC_FLAGS + ["-D" + d for d in defines] + ["-c", src, "-o", obj], obj + ".log"))
     for s in CPP_SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(OUT_DIR, s + ".o")
+        obj = os.path.join(out_dir, s + ".o")
         objs.append(obj)
         if force or _stale(obj, src):
             jobs.append((["g++"] + CXX_FLAGS + ["-c", src, "-o", obj], obj + ".log"))
@@ -72,10 +74,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             for o in outs:
                 sys.stdout.write(o)
-    if jobs or force or not os.path.exists(LIB):
-        _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs +
-             ["-lcudart_static", "-lrt", "-lpthread", "-ldl"], os.path.join(OUT_DIR, "link.log"))
-    return LIB
+    if jobs or force or not os.path.exists(lib):
+        _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", lib] + objs +
+             ["-lcudart_static", "-lrt", "-lpthread", "-ldl"], os.path.join(out_dir, "link.log"))
+    return lib
 
 
 if __name__ == "__main__":

@@ -27,6 +27,17 @@
 #include "engine.h"
 #include "ich.cuh"
 
+// Blocks of 128 lanes the batched kernel is compiled to fit per SM (register
+// budget); 0 = no constraint.
+#ifndef SVG_ICH_MIN_BLOCKS
+#define SVG_ICH_MIN_BLOCKS 0
+#endif
+#if SVG_ICH_MIN_BLOCKS > 0
+#define SVG_ICH_BOUNDS __launch_bounds__(128, SVG_ICH_MIN_BLOCKS)
+#else
+#define SVG_ICH_BOUNDS __launch_bounds__(128)
+#endif
+
 namespace svgb {
 
 struct PhaseOut {
@@ -126,7 +137,7 @@ __device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
     if (L.flags & kFlagUndefined) O.st_flags[v] |= 8;
 }
 
-__global__ void __launch_bounds__(128) k_ich_batched(LaneConfig C, PhaseOut O) {
+__global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
     int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     Lane L(C, gtid);
     int r = atomicAdd(O.work, 1);
@@ -395,21 +406,24 @@ __global__ void k_iota(int32_t* o, int32_t n, int32_t base) {
 namespace {
 
 struct Layout {
-    int32_t lanes = 0, wcap = 0, pcap = 0, vcap_log2 = 0, scap_log2 = 0, vlimit = 0;
+    int32_t lanes = 0, wphys = 0, pphys = 0, vcap_log2 = 0, scap_log2 = 0, vlimit = 0;
     bool operator==(const Layout& o) const {
-        return lanes == o.lanes && wcap == o.wcap && pcap == o.pcap && vcap_log2 == o.vcap_log2 &&
+        return lanes == o.lanes && wphys == o.wphys && pphys == o.pphys && vcap_log2 == o.vcap_log2 &&
                scap_log2 == o.scap_log2 && vlimit == o.vlimit;
     }
 };
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+// heap entries per lane: the sift-down reads up to index cap + 3
+int heap_stride(int cap) { return (cap + 4 + 3) / 4 * 4; }
+
 size_t lane_bytes(const Layout& l) {
     size_t b = 0;
-    b += (size_t)(l.wcap + 1) * sizeof(WinEntry);
-    b += (size_t)l.wcap * sizeof(WinPay);
-    b += (size_t)l.wcap * sizeof(uint16_t);
-    b += (size_t)(l.pcap + 1) * sizeof(PsEntry);
+    b += (size_t)heap_stride(l.wphys) * sizeof(WinEntry);
+    b += (size_t)l.wphys * sizeof(WinPay);
+    b += (size_t)l.wphys * sizeof(uint16_t);
+    b += (size_t)heap_stride(l.pphys) * sizeof(PsEntry);
     b += ((size_t)1 << l.vcap_log2) * sizeof(VSlot);
     b += (size_t)l.vlimit * sizeof(int32_t);
     b += ((size_t)1 << l.scap_log2) * sizeof(SSlot);
@@ -428,10 +442,10 @@ Arena g_arena[2];  // [0] main pass, [1] retry pass with larger tables
 void carve(Arena& A, const Layout& l, LaneConfig& C, cudaStream_t st) {
     size_t lanes = (size_t)l.lanes;
     size_t sz[7] = {
-        align_up(lanes * (l.wcap + 1) * sizeof(WinEntry)),
-        align_up(lanes * l.wcap * sizeof(WinPay)),
-        align_up(lanes * l.wcap * sizeof(uint16_t)),
-        align_up(lanes * (l.pcap + 1) * sizeof(PsEntry)),
+        align_up(lanes * heap_stride(l.wphys) * sizeof(WinEntry)),
+        align_up(lanes * l.wphys * sizeof(WinPay)),
+        align_up(lanes * l.wphys * sizeof(uint16_t)),
+        align_up(lanes * heap_stride(l.pphys) * sizeof(PsEntry)),
         align_up(lanes * ((size_t)1 << l.vcap_log2) * sizeof(VSlot)),
         align_up(lanes * l.vlimit * sizeof(int32_t)),
         align_up(lanes * ((size_t)1 << l.scap_log2) * sizeof(SSlot)),
@@ -492,12 +506,20 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     C.K = K;
     C.wcap = o.win_queue_cap;
     C.pcap = o.pseudo_queue_cap;
+    // Physical heaps of the first pass sized by K (observed high-water marks:
+    // windows ~2.3K, pseudo-sources ~0.7K); a source that needs more is re-run
+    // by the retry pass with physical = logical capacity.  The plain build
+    // always uses the full capacity.
+    C.wphys = plain ? C.wcap : std::min<int32_t>(C.wcap, std::max<int32_t>(128, (3 * K + 63) / 64 * 64));
+    C.pphys = plain ? C.pcap : std::min<int32_t>(C.pcap, std::max<int32_t>(64, (K + 63) / 64 * 64));
+    C.wstride = heap_stride(C.wphys);
+    C.pstride = heap_stride(C.pphys);
     C.vref = (uint32_t)K * o.vert_coef;
     C.sref = (uint32_t)K * o.split_coef;
     C.watchdog = (int64_t)1 << 26;
     Layout lay;
-    lay.wcap = C.wcap;
-    lay.pcap = C.pcap;
+    lay.wphys = C.wphys;
+    lay.pphys = C.pphys;
     lay.vcap_log2 = std::max(6, ilog2_ceil(2 * ((int64_t)C.vref + 1)));
     lay.scap_log2 = std::max(8, ilog2_ceil(4 * (int64_t)K));
     lay.vlimit = (int32_t)(((int64_t)3 << lay.vcap_log2) / 4);
@@ -537,7 +559,17 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     DevBuf b_order, b_misc, b_cand, b_candstart;
     b_order.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1));
     int32_t* d_order = b_order.as<int32_t>();
-    if (nsrc > 0) k_iota<<<(nsrc + 255) / 256, 256, 0, st>>>(d_order, nsrc, sb);
+    bool ordered = false;
+    if (!plain && o.heavy_first && m->cost_K == K && (int32_t)m->cost.size() == nv && nsrc > 0) {
+        std::vector<int32_t> ord((size_t)nsrc);
+        for (int32_t i = 0; i < nsrc; ++i) ord[(size_t)i] = sb + i;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int32_t a, int32_t b) { return m->cost[(size_t)a] > m->cost[(size_t)b]; });
+        SVG_CUDA(cudaMemcpyAsync(d_order, ord.data(), sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, st));
+        SVG_CUDA(cudaStreamSynchronize(st));
+        ordered = true;
+    }
+    if (nsrc > 0 && !ordered) k_iota<<<(nsrc + 255) / 256, 256, 0, st>>>(d_order, nsrc, sb);
     // misc: work, retry_n, acc[8], cand_used ; retry list ; cand_n ; deg
     // retry list: room for the first pass's failures and, after them, the retry pass's
     size_t retry_bytes = align_up(sizeof(int32_t) * 2 * (size_t)std::max(nsrc, 1));
@@ -625,7 +657,13 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
             if (retry_n > 0) {
                 // Sources whose tables filled: rerun them with 2x vertex and 4x split tables.
                 LaneConfig C2 = C;
+                C2.wphys = C.wcap;
+                C2.pphys = C.pcap;
+                C2.wstride = heap_stride(C2.wphys);
+                C2.pstride = heap_stride(C2.pphys);
                 Layout l2 = lay;
+                l2.wphys = C2.wphys;
+                l2.pphys = C2.pphys;
                 l2.vcap_log2 = retry_host_cap_log2_v;
                 l2.scap_log2 = retry_host_cap_log2_s;
                 l2.vlimit = (int32_t)(((int64_t)3 << l2.vcap_log2) / 4);
@@ -745,9 +783,18 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     S.launches = launches;
     S.scratch_bytes = scratch_bytes;
     (void)t03;
-    // flag tallies
+    // flag tallies; per-source costs kept on the mesh for the next build's order
     std::vector<int32_t> fl((size_t)nv);
     SVG_CUDA(cudaMemcpy(fl.data(), g->st_flags, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
+    if (!plain) {
+        std::vector<int32_t> w((size_t)nv);
+        SVG_CUDA(cudaMemcpy(w.data(), g->st_windows, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
+        if (m->cost_K != K || (int32_t)m->cost.size() != nv) {
+            m->cost.assign((size_t)nv, 0);
+            m->cost_K = K;
+        }
+        for (int32_t v = sb; v < se; ++v) m->cost[(size_t)v] = w[(size_t)v];
+    }
     for (int32_t f : fl) {
         if (f & 1) ++S.queue_drop_sources;
         if (f & 2) ++S.ref_overflow_sources;
@@ -792,10 +839,11 @@ constexpr int kStaticVlimit = 384;
 constexpr int kStaticSlimit = 384;
 
 constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
-constexpr size_t kSzWheap = al256((size_t)kStaticLanes * (kStaticWcap + 1) * sizeof(WinEntry));
+constexpr int kStaticStride = (kStaticWcap + 4 + 3) / 4 * 4;  // heap entries per lane
+constexpr size_t kSzWheap = al256((size_t)kStaticLanes * kStaticStride * sizeof(WinEntry));
 constexpr size_t kSzWpool = al256((size_t)kStaticLanes * kStaticWcap * sizeof(WinPay));
 constexpr size_t kSzWfree = al256((size_t)kStaticLanes * kStaticWcap * sizeof(uint16_t));
-constexpr size_t kSzPheap = al256((size_t)kStaticLanes * (kStaticPcap + 1) * sizeof(PsEntry));
+constexpr size_t kSzPheap = al256((size_t)kStaticLanes * kStaticStride * sizeof(PsEntry));
 constexpr size_t kSzVtab = al256((size_t)kStaticLanes * ((size_t)1 << kStaticVcapLog2) * sizeof(VSlot));
 constexpr size_t kSzVlist = al256((size_t)kStaticLanes * kStaticVlimit * sizeof(int32_t));
 constexpr size_t kSzStab = al256((size_t)kStaticLanes * ((size_t)1 << kStaticScapLog2) * sizeof(SSlot));
@@ -893,6 +941,10 @@ extern "C" svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t sour
         C.K = K;
         C.wcap = kStaticWcap;
         C.pcap = kStaticPcap;
+        C.wphys = kStaticWcap;
+        C.pphys = kStaticPcap;
+        C.wstride = kStaticStride;
+        C.pstride = kStaticStride;
         C.vref = (uint32_t)K * 2;
         C.sref = (uint32_t)K * 10;
         C.vcap_log2 = kStaticVcapLog2;

@@ -58,6 +58,11 @@ struct MeshDev {
 struct svg_mesh {
     svgb::HostMesh h;
     svgb::MeshDev d;
+    // Per-source cost (windows propagated) measured by the last batched build
+    // at K = cost_K: the next build at the same K orders its work queue
+    // heaviest first (longest-processing-time first).
+    int32_t cost_K = 0;
+    std::vector<int32_t> cost;
 };
 
 struct svg_graph {

@@ -10,8 +10,10 @@
 // Per-lane state lives in global memory (L1/L2-cached), sized per lane:
 //   window heap : 16-byte {key, psrc, slot|birth} entries, 1-based binary
 //                 min-heap with the reference's sift rules
-//                 (PriorityQueue.cuh:48-105), interleaved across the 32 lanes
-//                 of a warp so index i of all lanes is one 512-byte span;
+//                 (PriorityQueue.cuh:48-105), one contiguous array per lane:
+//                 the children 2i, 2i+1 of a node share one 32-byte sector and
+//                 its grandchildren 4i..4i+3 one 64-byte span, so a sift-down
+//                 fetches two levels per dependent memory round trip;
 //   window pool : 48-byte payloads addressed by slot, recycled via a stack;
 //   pseudo heap : 16-byte {key, vert, level<<8|birth} entries, same heap;
 //   vertex table: 32-byte slots, open addressing, epoch-stamped (no clears);
@@ -47,7 +49,7 @@ struct alignas(16) WinPay {
     double b0, b1;  // interval on the half-edge
     double sx, sy;  // unfolded (pseudo-)source, FlatenedSrc (ICHDevice.cuh:41-49)
     double psd;     // pseudoSrcDist
-    int32_t edge;
+    int32_t cross;  // twin of the window's half-edge: where it propagates (-1: boundary)
     int32_t level;
 };
 struct alignas(16) PsEntry {
@@ -89,7 +91,10 @@ struct alignas(8) PathEnd {
 struct LaneConfig {
     DevMesh M;
     int32_t K;
-    int32_t wcap, pcap;      // queue capacities (logical = physical)
+    int32_t wcap, pcap;      // logical queue capacities: pushes beyond them are dropped (reference)
+    int32_t wphys, pphys;    // physical heap capacities (<= logical); exceeding one hands the
+                             // source to the retry pass, which runs with physical = logical
+    int32_t wstride, pstride;// heap entries per lane (>= phys + 4, multiple of 4)
     uint32_t vref, sref;     // the reference's table sizes, K*vert_coef and K*split_coef
     int32_t vcap_log2, scap_log2;
     int32_t vlimit, slimit;  // max keys this lane's tables take before kFlagCapacity
@@ -184,19 +189,18 @@ struct Lane {
     int64_t steps;
 
     __device__ Lane(const LaneConfig& c, int gtid) : C(c) {
-        int warp = gtid >> 5, lane = gtid & 31;
-        WH = C.wheap + (size_t)warp * (C.wcap + 1) * 32 + lane;
-        PH = C.pheap + (size_t)warp * (C.pcap + 1) * 32 + lane;
-        WP = C.wpool + (size_t)gtid * C.wcap;
-        WF = C.wfree + (size_t)gtid * C.wcap;
+        WH = C.wheap + (size_t)gtid * C.wstride;
+        PH = C.pheap + (size_t)gtid * C.pstride;
+        WP = C.wpool + (size_t)gtid * C.wphys;
+        WF = C.wfree + (size_t)gtid * C.wphys;
         VT = C.vtab + ((size_t)gtid << C.vcap_log2);
         VL = C.vlist + (size_t)gtid * C.vlimit;
         ST = C.stab + ((size_t)gtid << C.scap_log2);
         epoch = C.epochs[gtid];
     }
 
-    __device__ __forceinline__ WinEntry& wh(int i) { return WH[(size_t)i << 5]; }
-    __device__ __forceinline__ PsEntry& ph(int i) { return PH[(size_t)i << 5]; }
+    __device__ __forceinline__ WinEntry& wh(int i) { return WH[i]; }
+    __device__ __forceinline__ PsEntry& ph(int i) { return PH[i]; }
 
     // ---------------------------------------------------------- tables
     __device__ __forceinline__ uint32_t vhash(uint32_t k) const { return (k * 0x9E3779B1u) >> (32 - C.vcap_log2); }
@@ -210,6 +214,39 @@ struct Lane {
             if (ke.y != epoch) return -1;
             if (ke.x == (uint32_t)v) return (int)h;
             h = (h + 1) & mask;
+        }
+    }
+    // First probe of a lookup, issued without waiting: slot key/epoch/enter/birth
+    // and the distance (one 32-byte sector).  vfinish completes the probe chain.
+    __device__ __forceinline__ void vfirst(int v, uint32_t& h, int4& k, double& d) const {
+        h = vhash((uint32_t)v);
+        k = *reinterpret_cast<const int4*>(&VT[h]);
+        d = VT[h].dist;
+    }
+    __device__ __forceinline__ int vfinish(int v, uint32_t h, int4& k, double& d) const {
+        const uint32_t mask = (1u << C.vcap_log2) - 1;
+        for (;;) {
+            if ((uint32_t)k.y != epoch) { d = DBL_MAX; return -1; }
+            if ((uint32_t)k.x == (uint32_t)v) return (int)h;
+            h = (h + 1) & mask;
+            k = *reinterpret_cast<const int4*>(&VT[h]);
+            d = VT[h].dist;
+        }
+    }
+    __device__ __forceinline__ void sfirst(int e, uint32_t& h, int4& k, double2& dx) const {
+        h = shash((uint32_t)e);
+        k = *reinterpret_cast<const int4*>(&ST[h]);
+        dx = *reinterpret_cast<const double2*>(&ST[h].dist);
+    }
+    // returns the slot or -1; dx = {dist, x} of the entry, {DBL_MAX, DBL_MAX} if absent
+    __device__ __forceinline__ int sfinish(int e, uint32_t h, int4& k, double2& dx) const {
+        const uint32_t mask = (1u << C.scap_log2) - 1;
+        for (;;) {
+            if ((uint32_t)k.y != epoch) { dx.x = DBL_MAX; dx.y = DBL_MAX; return -1; }
+            if ((uint32_t)k.x == (uint32_t)e) return (int)h;
+            h = (h + 1) & mask;
+            k = *reinterpret_cast<const int4*>(&ST[h]);
+            dx = *reinterpret_cast<const double2*>(&ST[h].dist);
         }
     }
     __device__ __forceinline__ double vdist(int v) {
@@ -290,6 +327,10 @@ struct Lane {
             flags |= kFlagQueueDrop;
             return;
         }
+        if (wsize >= C.wphys) {  // beyond this lane's physical heap: retry with a full one
+            flags |= kFlagCapacity;
+            return;
+        }
         int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
         WP[slot] = w.p;
         int cur = ++wsize, p = cur >> 1;
@@ -305,33 +346,49 @@ struct Lane {
         wh(cur) = e;
         if (wsize > maxw) maxw = wsize;
     }
+    // Pop with the reference's sift-down (PriorityQueue.cuh:76-105): children
+    // of `cur` are compared with each other (ties go right), the smaller moves
+    // up while it is smaller than the last element.  The children and
+    // grandchildren of `cur` are loaded together, so two levels cost one
+    // dependent round trip; reads past the heap's end stay inside the lane's
+    // array (stride >= cap + 4) and are never used.
     __device__ WinEntry wpop() {
-        WinEntry top = wh(1);
-        WinEntry last = wh(wsize);
-        --wsize;
+        WinEntry top = WH[1];
+        WinEntry last = WH[wsize];
+        const int n = --wsize;
         int cur = 1;
         for (;;) {
-            int l = cur << 1, r = l + 1, mc;
+            const int l = cur << 1;
+            if (l > n) break;
+            const WinEntry a = WH[l], b = WH[l + 1];
+            const int g = cur << 2;
+            WinEntry q0, q1, q2, q3;
+            if (g <= n) { q0 = WH[g]; q1 = WH[g + 1]; q2 = WH[g + 2]; q3 = WH[g + 3]; }
+            int mc;
             WinEntry ce;
-            if (r <= wsize) {
-                WinEntry a = wh(l), b = wh(r);
-                if (a.key < b.key) { mc = l; ce = a; } else { mc = r; ce = b; }
-            } else if (l <= wsize) {
-                mc = l; ce = wh(l);
-            } else {
-                break;
-            }
+            if (l + 1 <= n && !(a.key < b.key)) { mc = l + 1; ce = b; } else { mc = l; ce = a; }
             if (!(ce.key < last.key)) break;
-            wh(cur) = ce;
+            WH[cur] = ce;
+            cur = mc;
+            const int l2 = cur << 1;
+            if (l2 > n) break;
+            const WinEntry c0 = (mc == l) ? q0 : q2, c1 = (mc == l) ? q1 : q3;
+            if (l2 + 1 <= n && !(c0.key < c1.key)) { mc = l2 + 1; ce = c1; } else { mc = l2; ce = c0; }
+            if (!(ce.key < last.key)) break;
+            WH[cur] = ce;
             cur = mc;
         }
-        wh(cur) = last;
+        WH[cur] = last;
         WF[nfree++] = (uint16_t)(top.sb & 0xFFFF);
         return top;
     }
     __device__ void ppush(double key, int vert, int level, int birth) {
         if (psize >= C.pcap) {
             flags |= kFlagQueueDrop;
+            return;
+        }
+        if (psize >= C.pphys) {
+            flags |= kFlagCapacity;
             return;
         }
         int cur = ++psize, p = cur >> 1;
@@ -348,26 +405,32 @@ struct Lane {
         if (psize > maxp) maxp = psize;
     }
     __device__ PsEntry ppop() {
-        PsEntry top = ph(1);
-        PsEntry last = ph(psize);
-        --psize;
+        PsEntry top = PH[1];
+        PsEntry last = PH[psize];
+        const int n = --psize;
         int cur = 1;
         for (;;) {
-            int l = cur << 1, r = l + 1, mc;
+            const int l = cur << 1;
+            if (l > n) break;
+            const PsEntry a = PH[l], b = PH[l + 1];
+            const int g = cur << 2;
+            PsEntry q0, q1, q2, q3;
+            if (g <= n) { q0 = PH[g]; q1 = PH[g + 1]; q2 = PH[g + 2]; q3 = PH[g + 3]; }
+            int mc;
             PsEntry ce;
-            if (r <= psize) {
-                PsEntry a = ph(l), b = ph(r);
-                if (a.key < b.key) { mc = l; ce = a; } else { mc = r; ce = b; }
-            } else if (l <= psize) {
-                mc = l; ce = ph(l);
-            } else {
-                break;
-            }
+            if (l + 1 <= n && !(a.key < b.key)) { mc = l + 1; ce = b; } else { mc = l; ce = a; }
             if (!(ce.key < last.key)) break;
-            ph(cur) = ce;
+            PH[cur] = ce;
+            cur = mc;
+            const int l2 = cur << 1;
+            if (l2 > n) break;
+            const PsEntry c0 = (mc == l) ? q0 : q2, c1 = (mc == l) ? q1 : q3;
+            if (l2 + 1 <= n && !(c0.key < c1.key)) { mc = l2 + 1; ce = c1; } else { mc = l2; ce = c0; }
+            if (!(ce.key < last.key)) break;
+            PH[cur] = ce;
             cur = mc;
         }
-        ph(cur) = last;
+        PH[cur] = last;
         return top;
     }
 
@@ -416,7 +479,7 @@ struct Lane {
             HeRec hp = ld_he(M.he, prv(cur));
             NewWin w;
             finish_window(0.0, ho.len, hc.len, hp.len, 0.0, w);
-            w.p.edge = op;
+            w.p.cross = ho.twin;
             w.p.level = 0;
             wpush(w, source, 0);
             int opv = hc.v1;
@@ -446,31 +509,27 @@ struct Lane {
         VT[s].enter = -1;
     }
 
-    // ICHDevice::IsValidWindow (ICHDevice.cu:906-955).  v1, v2, v3: start,
-    // end and opposite vertex of the window's half-edge; l0 its length;
-    // (tx,ty) the opposite vertex in the window's frame.
-    __device__ bool is_valid(const NewWin& w, bool isLeft, int v1, int v2, int v3, double l0, double tx, double ty) {
+    // ICHDevice::IsValidWindow (ICHDevice.cu:906-955) given the distances d1,
+    // d2, d3 of the window half-edge's start, end and opposite vertex; l0 its
+    // length; (tx,ty) the opposite vertex in the window's frame.
+    __device__ __forceinline__ bool valid_window(const NewWin& w, bool isLeft, double d1, double d2, double d3,
+                                                 double l0, double tx, double ty) const {
         const WinPay& p = w.p;
         if (p.b1 <= p.b0) return false;
-        double dB = hyp(p.sx - p.b1, p.sy - 0.0);
-        double dA = hyp(p.sx - p.b0, p.sy - 0.0);
-        double d1 = vdist(v1);
+        const double dB = hyp(p.sx - p.b1, p.sy - 0.0);
+        const double dA = hyp(p.sx - p.b0, p.sy - 0.0);
         if (p.psd + dB > d1 + p.b1 && (p.psd + dB) / (d1 + p.b1) - 1.0 > 0.0) return false;
-        double d2 = vdist(v2);
         if (p.psd + dA > d2 + l0 - p.b0 && (p.psd + dA) / (d2 + l0 - p.b0) - 1.0 > 0.0) return false;
-        double d3 = vdist(v3);
-        if (isLeft) {
-            double q = hyp(tx - p.b0, ty - 0.0);
-            if (p.psd + dA > d3 + q && (p.psd + dA) / (d3 + q) - 1.0 > 0.0) return false;
-        } else {
-            double q = hyp(tx - p.b1, ty - 0.0);
-            if (p.psd + dB > d3 + q && (p.psd + dB) / (d3 + q) - 1.0 > kRelErr) return false;
-        }
+        const double q = isLeft ? hyp(tx - p.b0, ty - 0.0) : hyp(tx - p.b1, ty - 0.0);
+        const double dd = isLeft ? dA : dB;
+        const double thr = isLeft ? 0.0 : kRelErr;
+        if (p.psd + dd > d3 + q && (p.psd + dd) / (d3 + q) - 1.0 > thr) return false;
         return true;
     }
 
-    // ICHDevice::BuildWindow (ICHDevice.cu:957-973)
-    __device__ __forceinline__ void build_window(const WinPay& f, int edge, double elen, double t0, double t1,
+    // ICHDevice::BuildWindow (ICHDevice.cu:957-973); (v0x,v0y)-(v1x,v1y) is the
+    // child's half-edge in the parent's frame, cross the twin of that half-edge.
+    __device__ __forceinline__ void build_window(const WinPay& f, int cross, double elen, double t0, double t1,
                                                  double v0x, double v0y, double v1x, double v1y, NewWin& w) {
         double b0 = (1 - t0) * elen, b1 = (1 - t1) * elen;
         double px = v0x * t0 + v1x * (1 - t0), py = v0y * t0 + v1y * (1 - t0);
@@ -479,82 +538,91 @@ struct Lane {
         py = v0y * t1 + v1y * (1 - t1);
         double d1 = hyp(f.sx - px, f.sy - py);
         finish_window(b0, b1, d0, d1, f.psd, w);
-        w.p.edge = edge;
+        w.p.cross = cross;
         w.p.level = f.level + 1;
     }
 
-    // ICHDevice::PropagateWindow (ICHDevice.cu:618-726)
+    // ICHDevice::PropagateWindow (ICHDevice.cu:618-726).  The face beyond the
+    // window is e0 -> e1 -> e2 (e0 = twin of the window's half-edge) with
+    // vertices A = v0(e0), B = v1(e0) and the opposite vertex C = v1(e1).  The
+    // child on e1 (B->C) tests its validity against B, C, A and the child on
+    // e2 (C->A) against C, A, B, so the three distances are probed once, in
+    // parallel with the split entry of e0, and both children are built by one
+    // code path: child 0 = left (frame (0,0)->apex), child 1 = right (frame
+    // apex->(l0,0)).
     __device__ void propagate(const WinPay& win, int psrc, int birth) {
         const DevMesh& M = C.M;
-        int e0 = ld_he(M.he, win.edge).twin;
+        const int e0 = win.cross;
         if (e0 == -1) return;
-        int e1 = nxt(e0), e2 = nxt(e1);
-        HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
-        int opv = h1.v1;
-        double sx = win.sx, sy = win.sy;
-        double l0 = h0.len;
-        double2 v2 = ld_apex(M.geo, e0);
-        double interX = v2.x - v2.y * (v2.x - sx) / (v2.y - sy);
-        NewWin L, R;
-        bool hasL = true, hasR = true;
+        const int e1 = nxt(e0), e2 = nxt(e1);
+        const HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
+        const double2 v2 = ld_apex(M.geo, e0);
+        const double2 top1 = ld_top(M.geo, e1), top2 = ld_top(M.geo, e2);
+        const int A = h0.v0, B = h0.v1, Cv = h1.v1;
+        uint32_t hA, hB, hC, hS;
+        int4 kA, kB, kC, kS;
+        double dA, dB, dC;
+        double2 sdx;
+        vfirst(A, hA, kA, dA);
+        vfirst(B, hB, kB, dB);
+        vfirst(Cv, hC, kC, dC);
+        sfirst(e0, hS, kS, sdx);
+        vfinish(A, hA, kA, dA);
+        vfinish(B, hB, kB, dB);
+        const int sC = vfinish(Cv, hC, kC, dC);
+        const int sS = sfinish(e0, hS, kS, sdx);
+
+        const double sx = win.sx, sy = win.sy;
+        const double l0 = h0.len;
+        const double interX = v2.x - v2.y * (v2.x - sx) / (v2.y - sy);
+        bool keep0 = true, keep1 = true, both = false;
         if (interX <= win.b0) {
-            hasL = false;
-            double t0 = isect(sx, sy, win.b0, 0.0, v2.x, v2.y, l0, 0.0);
-            double t1 = isect(sx, sy, win.b1, 0.0, v2.x, v2.y, l0, 0.0);
-            build_window(win, e2, h2.len, t0, t1, v2.x, v2.y, l0, 0.0, R);
-            double2 tp = ld_top(M.geo, e2);
-            if (!is_valid(R, false, h2.v0, h2.v1, h0.v1, h2.len, tp.x, tp.y)) hasR = false;
+            keep0 = false;  // right child only
         } else if (interX >= win.b1) {
-            hasR = false;
-            double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
-            double t1 = isect(sx, sy, win.b1, 0.0, 0.0, 0.0, v2.x, v2.y);
-            build_window(win, e1, h1.len, t0, t1, 0.0, 0.0, v2.x, v2.y, L);
-            double2 tp = ld_top(M.geo, e1);
-            if (!is_valid(L, true, h1.v0, h1.v1, h0.v0, h1.len, tp.x, tp.y)) hasL = false;
+            keep1 = false;  // left child only
         } else {
-            double direct = hyp(v2.x - sx, v2.y - sy);
-            double D = direct + win.psd;
-            int ss = sfind(e0);
-            double sd = ss < 0 ? DBL_MAX : ST[ss].dist;
+            both = true;
+            const double D = hyp(v2.x - sx, v2.y - sy) + win.psd;
+            const double sd = sdx.x;
             if (D > sd && D / sd - 1.0 > kRelErr) {  // one angle, one split
-                hasL = (ss < 0 ? DBL_MAX : ST[ss].x) < interX;
-                hasR = !hasL;
+                keep0 = sdx.y < interX;
+                keep1 = !keep0;
             } else {
                 if (D < sd) {
-                    int s = sput(e0);
+                    const int s = sS >= 0 ? sS : sput(e0);
                     if (s < 0) return;
                     ST[s].dist = D;
                     ST[s].psrc = psrc;
                     ST[s].x = l0 - interX;
                 }
-                int vs = vfind(opv);
-                double vd = vs < 0 ? DBL_MAX : VT[vs].dist;
-                if (D < vd) {
-                    if (vd == DBL_MAX) ++total;
-                    int s = vs < 0 ? vput(opv) : vs;
+                if (D < dC) {
+                    if (dC == DBL_MAX) ++total;
+                    const int s = sC >= 0 ? sC : vput(Cv);
                     if (s < 0) return;
-                    int b = (int)(signed char)(VT[s].birth + 1);
-                    set_birth(s, opv, b);
+                    const int b = (int)(signed char)((sC >= 0 ? kC.w : -1) + 1);
+                    set_birth(s, Cv, b);
                     VT[s].dist = D;
                     VT[s].enter = e0;
-                    if (__ldg(&M.vr[opv].flags) & kVertSaddleGT) ppush(D, opv, win.level + 1, b);
+                    dC = D;  // the children's tests read the updated distance
+                    if (__ldg(&M.vr[Cv].flags) & kVertSaddleGT) ppush(D, Cv, win.level + 1, b);
                 }
             }
-            if (hasL) {
-                double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
-                build_window(win, e1, h1.len, t0, 0.0, 0.0, 0.0, v2.x, v2.y, L);
-                double2 tp = ld_top(M.geo, e1);
-                if (!is_valid(L, true, h1.v0, h1.v1, h0.v0, h1.len, tp.x, tp.y)) hasL = false;
-            }
-            if (hasR) {
-                double t1 = isect(sx, sy, win.b1, 0.0, v2.x, v2.y, l0, 0.0);
-                build_window(win, e2, h2.len, 1.0, t1, v2.x, v2.y, l0, 0.0, R);
-                double2 tp = ld_top(M.geo, e2);
-                if (!is_valid(R, false, h2.v0, h2.v1, h0.v1, h2.len, tp.x, tp.y)) hasR = false;
-            }
         }
-        if (hasL) wpush(L, psrc, birth);
-        if (hasR) wpush(R, psrc, birth);
+        NewWin W0, W1;
+        if (keep0) {
+            const double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
+            const double t1 = both ? 0.0 : isect(sx, sy, win.b1, 0.0, 0.0, 0.0, v2.x, v2.y);
+            build_window(win, h1.twin, h1.len, t0, t1, 0.0, 0.0, v2.x, v2.y, W0);
+            keep0 = valid_window(W0, true, dB, dC, dA, h1.len, top1.x, top1.y);
+        }
+        if (keep1) {
+            const double t0 = both ? 1.0 : isect(sx, sy, win.b0, 0.0, v2.x, v2.y, l0, 0.0);
+            const double t1 = isect(sx, sy, win.b1, 0.0, v2.x, v2.y, l0, 0.0);
+            build_window(win, h2.twin, h2.len, t0, t1, v2.x, v2.y, l0, 0.0, W1);
+            keep1 = valid_window(W1, false, dC, dA, dB, h2.len, top2.x, top2.y);
+        }
+        if (keep0) wpush(W0, psrc, birth);
+        if (keep1) wpush(W1, psrc, birth);
     }
 
     // Fan walks of GenSubWinsForPseudoSrcFrom{Window,PseudoSrc}
@@ -628,7 +696,7 @@ struct Lane {
             HeRec hn = ld_he(M.he, nxt(we));
             NewWin w;
             finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
-            w.p.edge = we;
+            w.p.cross = hw.twin;
             w.p.level = plevel + 1;
             wpush(w, pv, pbirth);
             startEdge = hn.twin;
@@ -661,8 +729,15 @@ struct Lane {
         } while (cur != start && cur != -1);
     }
 
-    // One iteration of ICHDevice::Execute's loop (ICHDevice.cu:72-119).
-    // Returns true when the source is finished.
+    // One iteration of ICHDevice::Execute's loop (ICHDevice.cu:72-119),
+    // arranged so that every lane of a warp walks the same code: each step
+    // pops exactly one heap entry.  The reference first pops every outdated
+    // window, then every outdated pseudo-source (birth time no longer that of
+    // its pseudo-source vertex, :80-86), then processes the smaller top; here
+    // one outdated entry is popped per step, in the same order, which removes
+    // the same entries (those pops change nothing else), and a processing
+    // step follows once both tops are current.  Window pops, outdated or not,
+    // share one sift-down.  Returns true when the source is finished.
     __device__ bool step() {
         if (wsize == 0 && psize == 0) return true;
         if (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined)) return true;
@@ -670,37 +745,51 @@ struct Lane {
             flags |= kFlagWatchdog;
             return true;
         }
-        // stale tops: birth no longer matches the pseudo-source's
-        while (wsize > 0) {
-            WinEntry t = wh(1);
-            int b = (t.psrc == source) ? src_birth : vbirth(t.psrc);
-            if ((int)(signed char)(t.sb >> 16) == b) break;
-            wpop();
+        WinEntry wt;
+        PsEntry pt;
+        wt.key = 0.0; wt.psrc = 0; wt.sb = 0;
+        pt.key = 0.0; pt.vert = 0; pt.lb = 0;
+        if (wsize > 0) wt = WH[1];
+        if (psize > 0) pt = PH[1];
+        // both birth lookups issued together
+        const bool wlook = wsize > 0 && wt.psrc != source;
+        const bool plook = psize > 0;
+        uint32_t hw = 0, hp = 0;
+        int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
+        double dw = 0.0, dp = 0.0;
+        if (wlook) vfirst(wt.psrc, hw, kw, dw);
+        if (plook) vfirst(pt.vert, hp, kp, dp);
+        int wb = src_birth, pb = -1;
+        if (wlook) wb = vfinish(wt.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
+        if (plook) pb = vfinish(pt.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+        const bool wstale = wsize > 0 && (int)(signed char)(wt.sb >> 16) != wb;
+        const bool pstale = !wstale && psize > 0 && (int)(signed char)(pt.lb & 0xFF) != pb;
+        bool procW = false, procP = false;
+        if (!wstale && !pstale) {
+            if (wsize > 0 && (psize == 0 || wt.key < pt.key)) {
+                procW = true;
+            } else if (psize > 0 && (wsize == 0 || wt.key >= pt.key)) {
+                procP = true;
+            } else {
+                flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
+                return true;
+            }
         }
-        while (psize > 0) {
-            PsEntry t = ph(1);
-            if ((int)(signed char)(t.lb & 0xFF) == vbirth(t.vert)) break;
-            ppop();
-        }
-        double wk = wsize > 0 ? wh(1).key : 0.0;
-        double pk = psize > 0 ? ph(1).key : 0.0;
-        if (wsize > 0 && (psize == 0 || wk < pk)) {
-            WinEntry t = wpop();
-            WinPay p = WP[t.sb & 0xFFFF];
-            if (p.level > C.M.nf) return false;
+        WinPay pay;
+        if (procW) pay = WP[wt.sb & 0xFFFF];  // issued before the sift-down
+        if (wstale || procW) wpop();
+        if (pstale || procP) ppop();
+        if (procW) {
+            if (pay.level > C.M.nf) return false;
             ++windows;
-            propagate(p, t.psrc, (int)(signed char)(t.sb >> 16));
-        } else if (psize > 0 && (wsize == 0 || wk >= pk)) {
-            PsEntry t = ppop();
-            int level = (int)(t.lb >> 8);
+            propagate(pay, wt.psrc, (int)(signed char)(wt.sb >> 16));
+        } else if (procP) {
+            const int level = (int)(pt.lb >> 8);
             if (level >= C.M.nf) return false;
             ++pseudos;
-            gen_sub_wins(t.key, t.vert, level, (int)(signed char)(t.lb & 0xFF));
-        } else if (wsize > 0 || psize > 0) {
-            flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
-            return true;
+            gen_sub_wins(pt.key, pt.vert, level, (int)(signed char)(pt.lb & 0xFF));
         } else {
-            return true;
+            return false;  // an outdated entry was removed; nothing was processed
         }
         if (C.K != -1 && total >= C.K) return true;
         return false;
