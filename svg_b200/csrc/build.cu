@@ -79,6 +79,8 @@ __device__ void record_stats(const Lane& L, const PhaseOut& O, int v) {
 // hop already: through a vertex that is not the source (enterEdge starts at
 // the vertex, or a window chain whose pseudo-source is another vertex), or
 // through enterEdge -1.  A vertex at distance 0 has no key point at all.
+// The vertex list holds table slots and each vertex slot the split slot of
+// its enter edge, so the walk is direct loads, four entries at a time.
 __device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
     const DevMesh& M = L.C.M;
     if (L.flags & kFlagCapacity) {
@@ -94,30 +96,35 @@ __device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
         return;  // the host sees cand_used > cand_cap and reruns with a larger pool
     }
     int n = 0;
-    for (int i = 0; i < L.vcount; ++i) {
-        int u = L.VL[i];
-        int s = L.vfind(u);
-        double d = L.VT[s].dist;
-        if (d == DBL_MAX || u == v) continue;
-        Cand c;
-        c.u = u;
-        c.dist = d;
-        c.ee = -1;
-        c.x = 0.0;
-        bool direct;
-        if (d == 0.0) {
-            direct = true;
-        } else {
-            int enter = L.VT[s].enter;
-            if (enter == -1) {
+    for (int i0 = 0; i0 < L.vcount; i0 += 4) {
+        VSlot e[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (i0 + k < L.vcount) e[k] = L.VT[L.VL[i0 + k]];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (i0 + k >= L.vcount) break;
+            const int u = (int)e[k].key;
+            const double d = e[k].dist;
+            if (d == DBL_MAX || u == v) continue;
+            Cand c;
+            c.u = u;
+            c.dist = d;
+            c.ee = -1;
+            c.x = 0.0;
+            bool direct;
+            if (d == 0.0) {
+                direct = true;
+            } else if (e[k].enter == -1) {
                 direct = false;
             } else {
+                const int enter = e[k].enter;
                 HeRec h = ld_he(M.he, enter);
                 if (h.v0 == u) {
                     direct = (h.v1 == v);
                 } else {
-                    int ss = L.sfind(enter);
-                    int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
+                    const int ss = e[k].sslot >= 0 ? e[k].sslot : L.sfind(enter);
+                    const int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
                     if ((unsigned)psrc >= (unsigned)M.nv) {
                         L.flags |= kFlagUndefined;
                         direct = false;
@@ -128,8 +135,8 @@ __device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
                     }
                 }
             }
+            if (direct) O.cand[base + n++] = c;
         }
-        if (direct) O.cand[base + n++] = c;
     }
     O.cand_start[v] = (int64_t)base;
     O.cand_n[v] = n;
@@ -137,18 +144,57 @@ __device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
     if (L.flags & kFlagUndefined) O.st_flags[v] |= 8;
 }
 
+// Longest a lane waits for its action type to be chosen (iterations).
+#ifndef SVG_ICH_MAX_WAIT
+#define SVG_ICH_MAX_WAIT 8
+#endif
+
+// Persistent batched build.  Each lane runs one source at a time and pulls
+// the next from the device work queue.  Every iteration the warp votes: each
+// lane's next action is a window pop, a pseudo-source pop or "source done"
+// (export + start the next source); the action type held by the most lanes
+// runs, the other lanes wait - at most SVG_ICH_MAX_WAIT iterations, after
+// which the longest-waiting lane's type runs.  A lane's own sequence of
+// actions is unchanged; only when it takes them is, so the rare, long paths
+// (pseudo-source fans, exports) run with many lanes at once instead of one
+// lane while 31 idle.
 __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
-    int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     Lane L(C, gtid);
     int r = atomicAdd(O.work, 1);
     int v = r < O.nsrc ? O.order[r] : -1;
     if (v >= 0) L.begin(v, false);
-    while (v >= 0) {
-        if (L.step()) {
-            finish_batched(L, O, v);
-            r = atomicAdd(O.work, 1);
-            v = r < O.nsrc ? O.order[r] : -1;
-            if (v >= 0) L.begin(v, false);
+    int waited = 0;
+    for (;;) {
+        const int act = v >= 0 ? L.peek() : -1;
+        const unsigned m0 = __ballot_sync(kFull, act == Lane::kActWindow);
+        const unsigned m1 = __ballot_sync(kFull, act == Lane::kActPseudo);
+        const unsigned m2 = __ballot_sync(kFull, act == Lane::kActDone);
+        if ((m0 | m1 | m2) == 0) break;
+        const unsigned starving = __ballot_sync(kFull, act >= 0 && waited >= SVG_ICH_MAX_WAIT);
+        int chosen;
+        if (starving) {
+            chosen = __shfl_sync(kFull, act, __ffs(starving) - 1);
+        } else {
+            const int c0 = __popc(m0), c1 = __popc(m1), c2 = __popc(m2);
+            chosen = (c0 >= c1 && c0 >= c2) ? Lane::kActWindow : (c1 >= c2 ? Lane::kActPseudo : Lane::kActDone);
+        }
+        const unsigned amask = chosen == Lane::kActWindow ? m0 : (chosen == Lane::kActPseudo ? m1 : m2);
+        if (act == chosen) {
+            waited = 0;
+            if (chosen == Lane::kActWindow) {
+                L.act_window(amask);
+            } else if (chosen == Lane::kActPseudo) {
+                L.act_pseudo(amask);
+            } else {
+                finish_batched(L, O, v);
+                r = atomicAdd(O.work, 1);
+                v = r < O.nsrc ? O.order[r] : -1;
+                if (v >= 0) L.begin(v, false);
+            }
+        } else if (act >= 0) {
+            ++waited;
         }
     }
     L.save_epoch(gtid);
@@ -507,11 +553,11 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     C.wcap = o.win_queue_cap;
     C.pcap = o.pseudo_queue_cap;
     // Physical heaps of the first pass sized by K (observed high-water marks:
-    // windows ~2.3K, pseudo-sources ~0.7K); a source that needs more is re-run
+    // windows up to ~2.3K, pseudo-sources up to ~1.3K); a source that needs more is re-run
     // by the retry pass with physical = logical capacity.  The plain build
     // always uses the full capacity.
     C.wphys = plain ? C.wcap : std::min<int32_t>(C.wcap, std::max<int32_t>(128, (3 * K + 63) / 64 * 64));
-    C.pphys = plain ? C.pcap : std::min<int32_t>(C.pcap, std::max<int32_t>(64, (K + 63) / 64 * 64));
+    C.pphys = plain ? C.pcap : std::min<int32_t>(C.pcap, std::max<int32_t>(128, (K + K / 2 + 64 + 63) / 64 * 64));
     C.wstride = heap_stride(C.wphys);
     C.pstride = heap_stride(C.pphys);
     C.vref = (uint32_t)K * o.vert_coef;

@@ -18,7 +18,7 @@
 //   pseudo heap : 16-byte {key, vert, level<<8|birth} entries, same heap;
 //   vertex table: 32-byte slots, open addressing, epoch-stamped (no clears);
 //   split table : 32-byte slots, same scheme;
-//   vertex list : keys in insertion order (the emission walks only these).
+//   vertex list : table slots in insertion order (the emission walks only these).
 #pragma once
 
 #include <cfloat>
@@ -63,7 +63,8 @@ struct alignas(32) VSlot {
     int32_t enter;  // enterEdge
     int32_t birth;  // char birthTime, sign-extended
     double dist;
-    double pad;
+    int32_t sslot;  // split-table slot of `enter` when the vertex was reached through a window, else -1
+    int32_t pad;
 };
 struct alignas(32) SSlot {
     uint32_t key;
@@ -271,9 +272,9 @@ struct Lane {
             return -1;
         }
         VSlot s;
-        s.key = (uint32_t)v; s.epoch = epoch; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.pad = 0.0;
+        s.key = (uint32_t)v; s.epoch = epoch; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.sslot = -1; s.pad = 0;
         VT[h] = s;
-        VL[vcount] = v;
+        VL[vcount] = (int32_t)h;
         ++vcount;
         if ((uint32_t)vcount > C.vref) flags |= kFlagRefOverflow;
         return (int)h;
@@ -310,7 +311,7 @@ struct Lane {
     __device__ void clear_tables() {
         for (int i = 0; i < (1 << C.vcap_log2); ++i) {
             VSlot s;
-            s.key = 0xFFFFFFFFu; s.epoch = 0; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.pad = 0.0;
+            s.key = 0xFFFFFFFFu; s.epoch = 0; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.sslot = -1; s.pad = 0;
             VT[i] = s;
         }
         for (int i = 0; i < (1 << C.scap_log2); ++i) {
@@ -444,6 +445,8 @@ struct Lane {
         windows = pseudos = generated = maxw = maxp = 0;
         steps = 0;
         src_birth = 0;
+        done = false;
+        pk_valid = false;
         if (clear_all) {
             clear_tables();  // every slot now carries epoch 0 = empty
             epoch = 1;
@@ -493,6 +496,7 @@ struct Lane {
             set_birth(s, opv, 0);
             VT[s].dist = hc.len;
             VT[s].enter = hc.twin;
+            VT[s].sslot = -1;
             if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE)) {
                 cur = hc.twin;
                 if (cur != -1) cur = nxt(cur);
@@ -507,6 +511,7 @@ struct Lane {
         set_birth(s, source, 0);
         VT[s].dist = 0.0;
         VT[s].enter = -1;
+        VT[s].sslot = -1;
     }
 
     // ICHDevice::IsValidWindow (ICHDevice.cu:906-955) given the distances d1,
@@ -550,64 +555,95 @@ struct Lane {
     // parallel with the split entry of e0, and both children are built by one
     // code path: child 0 = left (frame (0,0)->apex), child 1 = right (frame
     // apex->(l0,0)).
-    __device__ void propagate(const WinPay& win, int psrc, int birth) {
+    // All lanes of `amask` call this together and meet at each __syncwarp, so
+    // the phases run converged; a lane with nothing to do (live == false, or a
+    // boundary edge, or a full table) only predicates its work off.
+    __device__ void propagate(const WinPay& win, int psrc, int birth, bool live, unsigned amask) {
         const DevMesh& M = C.M;
         const int e0 = win.cross;
-        if (e0 == -1) return;
-        const int e1 = nxt(e0), e2 = nxt(e1);
-        const HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
-        const double2 v2 = ld_apex(M.geo, e0);
-        const double2 top1 = ld_top(M.geo, e1), top2 = ld_top(M.geo, e2);
-        const int A = h0.v0, B = h0.v1, Cv = h1.v1;
-        uint32_t hA, hB, hC, hS;
-        int4 kA, kB, kC, kS;
-        double dA, dB, dC;
-        double2 sdx;
-        vfirst(A, hA, kA, dA);
-        vfirst(B, hB, kB, dB);
-        vfirst(Cv, hC, kC, dC);
-        sfirst(e0, hS, kS, sdx);
-        vfinish(A, hA, kA, dA);
-        vfinish(B, hB, kB, dB);
-        const int sC = vfinish(Cv, hC, kC, dC);
-        const int sS = sfinish(e0, hS, kS, sdx);
+        live = live && e0 != -1;
+        int e1 = 0, e2 = 0, A = 0, B = 0, Cv = 0;
+        HeRec h0, h1, h2;
+        double2 v2 = make_double2(0.0, 0.0), top1 = v2, top2 = v2;
+        uint32_t hA = 0, hB = 0, hC = 0, hS = 0;
+        int4 kA = make_int4(0, 0, 0, 0), kB = kA, kC = kA, kS = kA;
+        double dA = 0.0, dB = 0.0, dC = 0.0;
+        double2 sdx = v2;
+        int sC = -1, sS = -1;
+        if (live) {
+            e1 = nxt(e0);
+            e2 = nxt(e1);
+            h0 = ld_he(M.he, e0);
+            h1 = ld_he(M.he, e1);
+            h2 = ld_he(M.he, e2);
+            v2 = ld_apex(M.geo, e0);
+            top1 = ld_top(M.geo, e1);
+            top2 = ld_top(M.geo, e2);
+            A = h0.v0;
+            B = h0.v1;
+            Cv = h1.v1;
+            vfirst(A, hA, kA, dA);
+            vfirst(B, hB, kB, dB);
+            vfirst(Cv, hC, kC, dC);
+            sfirst(e0, hS, kS, sdx);
+            vfinish(A, hA, kA, dA);
+            vfinish(B, hB, kB, dB);
+            sC = vfinish(Cv, hC, kC, dC);
+            sS = sfinish(e0, hS, kS, sdx);
+        }
+        __syncwarp(amask);
 
         const double sx = win.sx, sy = win.sy;
         const double l0 = h0.len;
-        const double interX = v2.x - v2.y * (v2.x - sx) / (v2.y - sy);
-        bool keep0 = true, keep1 = true, both = false;
-        if (interX <= win.b0) {
-            keep0 = false;  // right child only
-        } else if (interX >= win.b1) {
-            keep1 = false;  // left child only
-        } else {
-            both = true;
-            const double D = hyp(v2.x - sx, v2.y - sy) + win.psd;
-            const double sd = sdx.x;
-            if (D > sd && D / sd - 1.0 > kRelErr) {  // one angle, one split
-                keep0 = sdx.y < interX;
-                keep1 = !keep0;
+        bool keep0 = live, keep1 = live, both = false;
+        double interX = 0.0;
+        if (live) {
+            interX = v2.x - v2.y * (v2.x - sx) / (v2.y - sy);
+            if (interX <= win.b0) {
+                keep0 = false;  // right child only
+            } else if (interX >= win.b1) {
+                keep1 = false;  // left child only
             } else {
-                if (D < sd) {
-                    const int s = sS >= 0 ? sS : sput(e0);
-                    if (s < 0) return;
-                    ST[s].dist = D;
-                    ST[s].psrc = psrc;
-                    ST[s].x = l0 - interX;
-                }
-                if (D < dC) {
-                    if (dC == DBL_MAX) ++total;
-                    const int s = sC >= 0 ? sC : vput(Cv);
-                    if (s < 0) return;
-                    const int b = (int)(signed char)((sC >= 0 ? kC.w : -1) + 1);
-                    set_birth(s, Cv, b);
-                    VT[s].dist = D;
-                    VT[s].enter = e0;
-                    dC = D;  // the children's tests read the updated distance
-                    if (__ldg(&M.vr[Cv].flags) & kVertSaddleGT) ppush(D, Cv, win.level + 1, b);
+                both = true;
+                const double D = hyp(v2.x - sx, v2.y - sy) + win.psd;
+                const double sd = sdx.x;
+                if (D > sd && D / sd - 1.0 > kRelErr) {  // one angle, one split
+                    keep0 = sdx.y < interX;
+                    keep1 = !keep0;
+                } else {
+                    int ssl = sS;
+                    bool ok = true;
+                    if (D < sd) {
+                        ssl = sS >= 0 ? sS : sput(e0);
+                        if (ssl < 0) {
+                            ok = false;  // table full: the source goes to the retry pass
+                        } else {
+                            ST[ssl].dist = D;
+                            ST[ssl].psrc = psrc;
+                            ST[ssl].x = l0 - interX;
+                        }
+                    }
+                    if (ok && D < dC) {
+                        if (dC == DBL_MAX) ++total;
+                        const int s = sC >= 0 ? sC : vput(Cv);
+                        if (s < 0) {
+                            ok = false;
+                        } else {
+                            const int b = (int)(signed char)((sC >= 0 ? kC.w : -1) + 1);
+                            set_birth(s, Cv, b);
+                            VT[s].dist = D;
+                            VT[s].enter = e0;
+                            VT[s].sslot = ssl;  // D < dC <= split distance: the entry was just written
+                            dC = D;  // the children's tests read the updated distance
+                            if (__ldg(&M.vr[Cv].flags) & kVertSaddleGT) ppush(D, Cv, win.level + 1, b);
+                        }
+                    }
+                    if (!ok) keep0 = keep1 = false;
                 }
             }
         }
+        __syncwarp(amask);
+
         NewWin W0, W1;
         if (keep0) {
             const double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
@@ -621,8 +657,11 @@ struct Lane {
             build_window(win, h2.twin, h2.len, t0, t1, v2.x, v2.y, l0, 0.0, W1);
             keep1 = valid_window(W1, false, dC, dA, dB, h2.len, top2.x, top2.y);
         }
+        __syncwarp(amask);
         if (keep0) wpush(W0, psrc, birth);
+        __syncwarp(amask);
         if (keep1) wpush(W1, psrc, birth);
+        __syncwarp(amask);
     }
 
     // Fan walks of GenSubWinsForPseudoSrcFrom{Window,PseudoSrc}
@@ -650,148 +689,193 @@ struct Lane {
         if (cur != -1) endEdge = ld_he(M.he, nxt(nxt(ld_he(M.he, cur).twin))).twin;
     }
 
-    // ICHDevice::GenSubWinsForPseudoSrc (ICHDevice.cu:728-793)
-    __device__ void gen_sub_wins(double pdist, int pv, int plevel, int pbirth) {
+    // ICHDevice::GenSubWinsForPseudoSrc (ICHDevice.cu:728-793).  Called by
+    // the lanes of `amask` together (see propagate); `live` predicates.
+    __device__ void gen_sub_wins(double pdist, int pv, int plevel, int pbirth, bool live, unsigned amask) {
         const DevMesh& M = C.M;
-        int vs = vfind(pv);
-        int enter = vs < 0 ? -1 : VT[vs].enter;
-        int vb = vs < 0 ? -1 : VT[vs].birth;
-        int startEdge, endEdge;
-        if (enter == -1 && vb != -1) {
-            startEdge = __ldg(&M.vr[pv].first);
-            endEdge = startEdge;
-        } else if (enter >= 0 && ld_he(M.he, enter).v0 == pv) {
-            fan_walk(enter, ld_he(M.he, enter).twin, 0.0, 0.0, startEdge, endEdge);
-        } else if (enter >= 0 && ld_he(M.he, nxt(enter)).v1 == pv) {
-            // GenSubWinsForPseudoSrcFromWindow (ICHDevice.cu:795-858)
-            int e0 = enter, e1 = nxt(e0), e2 = nxt(e1);
-            HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
-            double l0 = h0.len, l1 = h1.len, l2 = h2.len;
-            int ss = sfind(e0);
-            double sx = ss < 0 ? DBL_MAX : ST[ss].x;
-            double ex = l0 - sx, ey = 0.0;
-            double2 v2 = ld_apex(M.geo, e0);
-            double dx = ex - v2.x, dy = ey - v2.y;
-            double dl = hyp(dx, dy);
-            double a0 = (dx * (0.0 - v2.x) + dy * (0.0 - v2.y)) / dl / l1;
-            double a1 = (dx * (l0 - v2.x) + dy * (0.0 - v2.y)) / dl / l2;
-            if (a0 > 1.0) a0 = 1.0; else if (a0 < -1.0) a0 = -1.0;
-            if (a1 > 1.0) a1 = 1.0; else if (a1 < -1.0) a1 = -1.0;
-            a0 = acos(a0);
-            a1 = acos(a1);
-            fan_walk(h1.twin, h2.twin, a0, a1, startEdge, endEdge);
-        } else {
-            flags |= kFlagUndefined;  // assert(false) at ICHDevice.cu:740
-            return;
-        }
-        if (flags & kFlagWatchdog) return;
-        int guard = 0;
-        do {
-            if (startEdge < 0) {  // the reference reads edges[-1] here
-                flags |= kFlagUndefined;
-                break;
+        int startEdge = -1, endEdge = -1;
+        if (live) {
+            int vs = vfind(pv);
+            int enter = vs < 0 ? -1 : VT[vs].enter;
+            int vb = vs < 0 ? -1 : VT[vs].birth;
+            if (enter == -1 && vb != -1) {
+                startEdge = __ldg(&M.vr[pv].first);
+                endEdge = startEdge;
+            } else if (enter >= 0 && ld_he(M.he, enter).v0 == pv) {
+                fan_walk(enter, ld_he(M.he, enter).twin, 0.0, 0.0, startEdge, endEdge);
+            } else if (enter >= 0 && ld_he(M.he, nxt(enter)).v1 == pv) {
+                // GenSubWinsForPseudoSrcFromWindow (ICHDevice.cu:795-858)
+                int e0 = enter, e1 = nxt(e0), e2 = nxt(e1);
+                HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
+                double l0 = h0.len, l1 = h1.len, l2 = h2.len;
+                int ss = sfind(e0);
+                double sx = ss < 0 ? DBL_MAX : ST[ss].x;
+                double ex = l0 - sx, ey = 0.0;
+                double2 v2 = ld_apex(M.geo, e0);
+                double dx = ex - v2.x, dy = ey - v2.y;
+                double dl = hyp(dx, dy);
+                double a0 = (dx * (0.0 - v2.x) + dy * (0.0 - v2.y)) / dl / l1;
+                double a1 = (dx * (l0 - v2.x) + dy * (0.0 - v2.y)) / dl / l2;
+                if (a0 > 1.0) a0 = 1.0; else if (a0 < -1.0) a0 = -1.0;
+                if (a1 > 1.0) a1 = 1.0; else if (a1 < -1.0) a1 = -1.0;
+                a0 = acos(a0);
+                a1 = acos(a1);
+                fan_walk(h1.twin, h2.twin, a0, a1, startEdge, endEdge);
+            } else {
+                flags |= kFlagUndefined;  // assert(false) at ICHDevice.cu:740
+                live = false;
             }
-            int we = nxt(startEdge);
-            HeRec hs = ld_he(M.he, startEdge), hw = ld_he(M.he, we);
-            HeRec hn = ld_he(M.he, nxt(we));
-            NewWin w;
-            finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
-            w.p.cross = hw.twin;
-            w.p.level = plevel + 1;
-            wpush(w, pv, pbirth);
-            startEdge = hn.twin;
-            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
-        } while (startEdge != endEdge);
-
-        int start = __ldg(&M.vr[pv].first), cur = start;
-        guard = 0;
-        do {
-            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return; }
-            HeRec hc = ld_he(M.he, cur);
-            int opv = hc.v1;
-            int os = vfind(opv);
-            double od = os < 0 ? DBL_MAX : VT[os].dist;
-            if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE) || od < pdist + hc.len) {
+            if (flags & kFlagWatchdog) live = false;
+        }
+        __syncwarp(amask);
+        if (live) {
+            int guard = 0;
+            do {
+                if (startEdge < 0) {  // the reference reads edges[-1] here
+                    flags |= kFlagUndefined;
+                    break;
+                }
+                int we = nxt(startEdge);
+                HeRec hs = ld_he(M.he, startEdge), hw = ld_he(M.he, we);
+                HeRec hn = ld_he(M.he, nxt(we));
+                NewWin w;
+                finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
+                w.p.cross = hw.twin;
+                w.p.level = plevel + 1;
+                wpush(w, pv, pbirth);
+                startEdge = hn.twin;
+                if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
+            } while (startEdge != endEdge);
+        }
+        __syncwarp(amask);
+        if (live) {
+            int start = __ldg(&M.vr[pv].first), cur = start;
+            int guard = 0;
+            do {
+                if (++guard > 1 << 20) { flags |= kFlagWatchdog; break; }
+                HeRec hc = ld_he(M.he, cur);
+                int opv = hc.v1;
+                int os = vfind(opv);
+                double od = os < 0 ? DBL_MAX : VT[os].dist;
+                if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE) || od < pdist + hc.len) {
+                    cur = hc.twin;
+                    if (cur != -1) cur = nxt(cur);
+                    continue;
+                }
+                if (od == DBL_MAX) ++total;
+                int s = os < 0 ? vput(opv) : os;
+                if (s < 0) break;
+                VT[s].dist = pdist + hc.len;
+                int b = (int)(signed char)(VT[s].birth + 1);
+                set_birth(s, opv, b);
+                VT[s].enter = hc.twin;
+                VT[s].sslot = -1;
+                ppush(VT[s].dist, opv, plevel, b);
                 cur = hc.twin;
                 if (cur != -1) cur = nxt(cur);
-                continue;
-            }
-            if (od == DBL_MAX) ++total;
-            int s = os < 0 ? vput(opv) : os;
-            if (s < 0) return;
-            VT[s].dist = pdist + hc.len;
-            int b = (int)(signed char)(VT[s].birth + 1);
-            set_birth(s, opv, b);
-            VT[s].enter = hc.twin;
-            ppush(VT[s].dist, opv, plevel, b);
-            cur = hc.twin;
-            if (cur != -1) cur = nxt(cur);
-        } while (cur != start && cur != -1);
+            } while (cur != start && cur != -1);
+        }
+        __syncwarp(amask);
     }
 
     // One iteration of ICHDevice::Execute's loop (ICHDevice.cu:72-119),
-    // arranged so that every lane of a warp walks the same code: each step
-    // pops exactly one heap entry.  The reference first pops every outdated
-    // window, then every outdated pseudo-source (birth time no longer that of
-    // its pseudo-source vertex, :80-86), then processes the smaller top; here
-    // one outdated entry is popped per step, in the same order, which removes
+    // split into peek() - which entry comes off next - and act() - pop it
+    // and process it.  The reference first pops every outdated window, then
+    // every outdated pseudo-source (birth time no longer that of its
+    // pseudo-source vertex, :80-86), then processes the smaller top; here one
+    // outdated entry is popped per action, in the same order, which removes
     // the same entries (those pops change nothing else), and a processing
-    // step follows once both tops are current.  Window pops, outdated or not,
-    // share one sift-down.  Returns true when the source is finished.
-    __device__ bool step() {
-        if (wsize == 0 && psize == 0) return true;
-        if (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined)) return true;
+    // action follows once both tops are current.
+    //   kActWindow  pop the window top (outdated, or processed: PropagateWindow)
+    //   kActPseudo  pop the pseudo-source top (outdated, or GenSubWinsForPseudoSrc)
+    //   kActDone    the source is finished
+    // peek() caches its decision until act() runs, so a lane may wait.
+    enum { kActWindow = 0, kActPseudo = 1, kActDone = 2 };
+    bool done;
+    bool pk_valid;
+    int pk_act;
+    bool pk_proc;  // process (true) or just drop an outdated entry (false)
+    WinEntry pk_w;
+    PsEntry pk_p;
+
+    __device__ int peek() {
+        if (pk_valid) return pk_act;
+        pk_valid = true;
+        pk_proc = false;
+        if (done || (wsize == 0 && psize == 0) || (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined))) {
+            done = true;
+            return pk_act = kActDone;
+        }
         if (++steps > C.watchdog) {
             flags |= kFlagWatchdog;
-            return true;
+            done = true;
+            return pk_act = kActDone;
         }
-        WinEntry wt;
-        PsEntry pt;
-        wt.key = 0.0; wt.psrc = 0; wt.sb = 0;
-        pt.key = 0.0; pt.vert = 0; pt.lb = 0;
-        if (wsize > 0) wt = WH[1];
-        if (psize > 0) pt = PH[1];
+        pk_w.key = 0.0; pk_w.psrc = 0; pk_w.sb = 0;
+        pk_p.key = 0.0; pk_p.vert = 0; pk_p.lb = 0;
+        if (wsize > 0) pk_w = WH[1];
+        if (psize > 0) pk_p = PH[1];
         // both birth lookups issued together
-        const bool wlook = wsize > 0 && wt.psrc != source;
+        const bool wlook = wsize > 0 && pk_w.psrc != source;
         const bool plook = psize > 0;
         uint32_t hw = 0, hp = 0;
         int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
         double dw = 0.0, dp = 0.0;
-        if (wlook) vfirst(wt.psrc, hw, kw, dw);
-        if (plook) vfirst(pt.vert, hp, kp, dp);
+        if (wlook) vfirst(pk_w.psrc, hw, kw, dw);
+        if (plook) vfirst(pk_p.vert, hp, kp, dp);
         int wb = src_birth, pb = -1;
-        if (wlook) wb = vfinish(wt.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
-        if (plook) pb = vfinish(pt.vert, hp, kp, dp) < 0 ? -1 : kp.w;
-        const bool wstale = wsize > 0 && (int)(signed char)(wt.sb >> 16) != wb;
-        const bool pstale = !wstale && psize > 0 && (int)(signed char)(pt.lb & 0xFF) != pb;
-        bool procW = false, procP = false;
-        if (!wstale && !pstale) {
-            if (wsize > 0 && (psize == 0 || wt.key < pt.key)) {
-                procW = true;
-            } else if (psize > 0 && (wsize == 0 || wt.key >= pt.key)) {
-                procP = true;
-            } else {
-                flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
-                return true;
-            }
-        }
+        if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
+        if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+        const bool wstale = wsize > 0 && (int)(signed char)(pk_w.sb >> 16) != wb;
+        if (wstale) return pk_act = kActWindow;
+        const bool pstale = psize > 0 && (int)(signed char)(pk_p.lb & 0xFF) != pb;
+        if (pstale) return pk_act = kActPseudo;
+        pk_proc = true;
+        if (wsize > 0 && (psize == 0 || pk_w.key < pk_p.key)) return pk_act = kActWindow;
+        if (psize > 0 && (wsize == 0 || pk_w.key >= pk_p.key)) return pk_act = kActPseudo;
+        flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
+        done = true;
+        return pk_act = kActDone;
+    }
+
+    // Pop the window top; process it if peek() said so.  The lanes of amask
+    // call this together (each of them with its own top).
+    __device__ void act_window(unsigned amask) {
+        pk_valid = false;
+        const bool proc = pk_proc;
+        const WinEntry t = pk_w;
         WinPay pay;
-        if (procW) pay = WP[wt.sb & 0xFFFF];  // issued before the sift-down
-        if (wstale || procW) wpop();
-        if (pstale || procP) ppop();
-        if (procW) {
-            if (pay.level > C.M.nf) return false;
-            ++windows;
-            propagate(pay, wt.psrc, (int)(signed char)(wt.sb >> 16));
-        } else if (procP) {
-            const int level = (int)(pt.lb >> 8);
-            if (level >= C.M.nf) return false;
-            ++pseudos;
-            gen_sub_wins(pt.key, pt.vert, level, (int)(signed char)(pt.lb & 0xFF));
-        } else {
-            return false;  // an outdated entry was removed; nothing was processed
-        }
-        if (C.K != -1 && total >= C.K) return true;
+        pay.cross = -1;
+        pay.level = 0;
+        if (proc) pay = WP[t.sb & 0xFFFF];  // issued before the sift-down
+        wpop();
+        __syncwarp(amask);
+        const bool live = proc && !(pay.level > C.M.nf);
+        if (live) ++windows;
+        propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask);
+        if (live && C.K != -1 && total >= C.K) done = true;
+    }
+
+    __device__ void act_pseudo(unsigned amask) {
+        pk_valid = false;
+        const bool proc = pk_proc;
+        const PsEntry t = pk_p;
+        ppop();
+        __syncwarp(amask);
+        const int level = (int)(t.lb >> 8);
+        const bool live = proc && !(level >= C.M.nf);
+        if (live) ++pseudos;
+        gen_sub_wins(t.key, t.vert, level, (int)(signed char)(t.lb & 0xFF), live, amask);
+        if (live && C.K != -1 && total >= C.K) done = true;
+    }
+
+    // peek + act for one lane on its own; true when finished.
+    __device__ bool step() {
+        const unsigned self = 1u << (threadIdx.x & 31);
+        const int a = peek();
+        if (a == kActDone) return true;
+        if (a == kActWindow) act_window(self);
+        else act_pseudo(self);
         return false;
     }
 };
