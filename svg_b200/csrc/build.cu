@@ -567,7 +567,7 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     lay.wphys = C.wphys;
     lay.pphys = C.pphys;
     lay.vcap_log2 = std::max(6, ilog2_ceil(2 * ((int64_t)C.vref + 1)));
-    lay.scap_log2 = std::max(8, ilog2_ceil(4 * (int64_t)K));
+    lay.scap_log2 = std::max(8, ilog2_ceil(8 * (int64_t)K));  // split entries reach ~1.6x the vertices
     lay.vlimit = (int32_t)(((int64_t)3 << lay.vcap_log2) / 4);
     C.vcap_log2 = lay.vcap_log2;
     C.scap_log2 = lay.scap_log2;

@@ -322,6 +322,10 @@ struct Lane {
     }
 
     // ----------------------------------------------------------- heaps
+    // Push with the reference's sift-up (PriorityQueue.cuh:48-67): the new
+    // entry moves up while its parent's key is greater.  The first four
+    // ancestors are loaded together and the loop runs over registers, so the
+    // lanes of a warp stay together; deeper climbs continue one level at a time.
     __device__ void wpush(const NewWin& w, int psrc, int birth) {
         ++generated;  // counts attempts, like numOfWinGen
         if (wsize >= C.wcap) {  // PriorityQueue.cuh:53: dropped when full
@@ -332,19 +336,35 @@ struct Lane {
             flags |= kFlagCapacity;
             return;
         }
-        int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
+        const int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
         WP[slot] = w.p;
-        int cur = ++wsize, p = cur >> 1;
-        while (p > 0) {
-            WinEntry pe = wh(p);
-            if (!(pe.key > w.key)) break;
-            wh(cur) = pe;
+        int cur = ++wsize;
+        WinEntry anc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if ((cur >> (j + 1)) > 0) anc[j] = WH[cur >> (j + 1)];
+        int j = 0;
+        for (; j < 4; ++j) {
+            const int p = cur >> 1;
+            if (p == 0 || !(anc[j].key > w.key)) break;
+            WH[cur] = anc[j];
             cur = p;
-            p = cur >> 1;
+        }
+        if (j == 4) {
+            for (;;) {
+                const int p = cur >> 1;
+                if (p == 0) break;
+                const WinEntry pe = WH[p];
+                if (!(pe.key > w.key)) break;
+                WH[cur] = pe;
+                cur = p;
+            }
         }
         WinEntry e;
-        e.key = w.key; e.psrc = psrc; e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        wh(cur) = e;
+        e.key = w.key;
+        e.psrc = psrc;
+        e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
+        WH[cur] = e;
         if (wsize > maxw) maxw = wsize;
     }
     // Pop with the reference's sift-down (PriorityQueue.cuh:76-105): children
