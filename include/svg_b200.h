@@ -204,6 +204,12 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
 svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t source_begin, int32_t source_end,
                                  int32_t* d_tails, int32_t* d_adj, double* d_dist, void* stream);
 
+/* Device memory freed by the library (graphs, build scratch, query buffers)
+ * is cached for reuse; this returns all cached blocks to CUDA and reports how
+ * many bytes it released.  No counterpart in the reference (it cudaMallocs
+ * and cudaFrees every buffer). */
+size_t svg_trim_device_cache(void);
+
 /* Synchronise the library's stream; returns the device time in ms since the
  * previous svg_timer_mark (CUDA events on the library stream). */
 svg_status svg_timer_mark(double* ms_since_last);

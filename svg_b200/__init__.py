@@ -84,7 +84,7 @@ EXPORTS = [
     "svg_graph_stats", "svg_graph_source_stats", "svg_graph_free", "svg_graph_counts", "svg_graph_copy_csr",
     "svg_graph_copy_nodes", "svg_graph_device_csr", "svg_graph_save", "svg_graph_load", "svg_sssd_batch",
     "svg_msad_batch", "svg_sssd_batch_device", "svg_msad_batch_device", "svg_timer_mark",
-    "svg_build_rows_static",
+    "svg_build_rows_static", "svg_trim_device_cache",
 ]
 
 _lib = None
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
     L.svg_msad_batch_device.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P]
     L.svg_timer_mark.argtypes = [C.POINTER(C.c_double)]
     L.svg_build_rows_static.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P]
+    L.svg_trim_device_cache.restype = C.c_size_t
     _lib = L
     return L
 

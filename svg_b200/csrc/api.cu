@@ -2,7 +2,10 @@
 #include <cfloat>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <unordered_map>
 
 #include "engine.h"
 #include "ich.cuh"
@@ -22,22 +25,93 @@ cudaStream_t lib_stream() {
     return g_stream;
 }
 
-void DevBuf::reserve(size_t n) {
-    if (n <= bytes && p) return;
-    release();
-    if (n == 0) n = 16;
+namespace {
+struct Pool {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;      // size -> block
+    std::unordered_map<void*, size_t> live;        // block -> size
+    size_t cached = 0;
+};
+Pool& pool() {
+    static Pool* P = new Pool();  // never destroyed: blocks may be freed during process exit
+    return *P;
+}
+size_t round_block(size_t n) {
+    if (n < 16) n = 16;
+    if (n >= ((size_t)1 << 20)) return (n + ((size_t)2 << 20) - 1) / ((size_t)2 << 20) * ((size_t)2 << 20);
+    size_t b = 512;
+    while (b < n) b <<= 1;
+    return b;
+}
+}  // namespace
+
+void* dev_alloc(size_t bytes) {
+    Pool& P = pool();
+    const size_t n = round_block(bytes);
+    {
+        std::lock_guard<std::mutex> lk(P.mu);
+        auto it = P.free_blocks.lower_bound(n);
+        if (it != P.free_blocks.end() && it->first <= 2 * n) {  // reuse, wasting at most half
+            void* q = it->second;
+            size_t sz = it->first;
+            P.free_blocks.erase(it);
+            P.cached -= sz;
+            P.live[q] = sz;
+            return q;
+        }
+    }
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, n);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        throw SvgError{SVG_ERR_NOMEM, "cudaMalloc of " + std::to_string(n) + " bytes failed: " + cudaGetErrorString(e)};
+        dev_trim();
+        e = cudaMalloc(&q, n);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw SvgError{SVG_ERR_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed: " +
+                                              cudaGetErrorString(e)};
+        }
     }
-    p = q;
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.live[q] = n;
+    return q;
+}
+
+void dev_free(void* q) {
+    if (!q) return;
+    Pool& P = pool();
+    if (g_stream) cudaStreamSynchronize(g_stream);  // no kernel of the library still reads it
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.live.find(q);
+    if (it == P.live.end()) return;
+    P.free_blocks.emplace(it->second, q);
+    P.cached += it->second;
+    P.live.erase(it);
+}
+
+size_t dev_trim() {
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    size_t n = 0;
+    for (auto& kv : P.free_blocks) {
+        cudaFree(kv.second);
+        n += kv.first;
+    }
+    P.free_blocks.clear();
+    P.cached = 0;
+    return n;
+}
+
+void DevBuf::reserve(size_t n) {
+    if (n <= bytes && p) return;
+    release();
+    if (n == 0) n = 16;
+    p = dev_alloc(n);
     bytes = n;
 }
 
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
     p = nullptr;
     bytes = 0;
 }
@@ -59,10 +133,10 @@ void upload_mesh(svg_mesh* m) {
     const HostMesh& H = m->h;
     cudaStream_t st = lib_stream();
     MeshDev& D = m->d;
-    SVG_CUDA(cudaMalloc(&D.he, sizeof(HeRec) * (size_t)H.ne));
-    SVG_CUDA(cudaMalloc(&D.geo, sizeof(HeGeo) * (size_t)H.ne));
-    SVG_CUDA(cudaMalloc(&D.vr, sizeof(VertRec) * (size_t)H.nv));
-    SVG_CUDA(cudaMalloc(&D.pos, sizeof(double) * 3 * (size_t)H.nv));
+    D.he = dev_alloc_n<HeRec>((size_t)H.ne);
+    D.geo = dev_alloc_n<HeGeo>((size_t)H.ne);
+    D.vr = dev_alloc_n<VertRec>((size_t)H.nv);
+    D.pos = dev_alloc_n<double>(3 * (size_t)H.nv);
     SVG_CUDA(cudaMemcpyAsync(D.he, H.he.data(), sizeof(HeRec) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.geo, H.geo.data(), sizeof(HeGeo) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.vr, H.vr.data(), sizeof(VertRec) * (size_t)H.nv, cudaMemcpyHostToDevice, st));
@@ -76,11 +150,11 @@ void upload_mesh(svg_mesh* m) {
 
 void free_graph_device(svg_graph* g) {
     if (!g) return;
-    cudaFree(g->off);
-    cudaFree(g->adj);
-    cudaFree(g->dist);
-    cudaFree(g->paths);
-    cudaFree(g->st_windows);
+    dev_free(g->off);
+    dev_free(g->adj);
+    dev_free(g->dist);
+    dev_free(g->paths);
+    dev_free(g->st_windows);
     g->off = nullptr;
     g->adj = nullptr;
     g->dist = nullptr;
@@ -165,10 +239,10 @@ svg_status svg_mesh_upload(svg_mesh* m) {
 
 void svg_mesh_free(svg_mesh* m) {
     if (!m) return;
-    cudaFree(m->d.he);
-    cudaFree(m->d.geo);
-    cudaFree(m->d.vr);
-    cudaFree(m->d.pos);
+    dev_free(m->d.he);
+    dev_free(m->d.geo);
+    dev_free(m->d.vr);
+    dev_free(m->d.pos);
     delete m;
 }
 
@@ -401,10 +475,10 @@ svg_status svg_graph_load(svg_mesh* m, int32_t K, const char* path, svg_graph** 
                                 nodes[i].next_to_dst_x};
             }
             size_t E = std::max<size_t>(nodes.size(), 1);
-            SVG_CUDA(cudaMalloc(&g->off, sizeof(int64_t) * off.size()));
-            SVG_CUDA(cudaMalloc(&g->adj, sizeof(int32_t) * E));
-            SVG_CUDA(cudaMalloc(&g->dist, sizeof(double) * E));
-            SVG_CUDA(cudaMalloc(&g->paths, sizeof(PathEnd) * E));
+            g->off = dev_alloc_n<int64_t>(off.size());
+            g->adj = dev_alloc_n<int32_t>(E);
+            g->dist = dev_alloc_n<double>(E);
+            g->paths = dev_alloc(sizeof(PathEnd) * E);
             SVG_CUDA(cudaMemcpy(g->off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
             if (!nodes.empty()) {
                 SVG_CUDA(cudaMemcpy(g->adj, adj.data(), sizeof(int32_t) * adj.size(), cudaMemcpyHostToDevice));
@@ -497,6 +571,8 @@ svg_status svg_msad_batch(svg_graph* g, int32_t n, const int64_t* set_offsets, c
         return SVG_OK;
     });
 }
+
+size_t svg_trim_device_cache(void) { return dev_trim(); }
 
 svg_status svg_timer_mark(double* ms_since_last) {
     return guarded([&]() -> svg_status {

@@ -544,8 +544,12 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
 
     int dev = 0;
     SVG_CUDA(cudaGetDevice(&dev));
-    cudaDeviceProp prop;
-    SVG_CUDA(cudaGetDeviceProperties(&prop, dev));
+    static thread_local int prop_dev = -1;
+    static thread_local cudaDeviceProp prop;
+    if (prop_dev != dev) {
+        SVG_CUDA(cudaGetDeviceProperties(&prop, dev));
+        prop_dev = dev;
+    }
 
     LaneConfig C{};
     C.M = m->d.view();
@@ -634,11 +638,11 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     g->nv = nv;
     g->K = K;
     g->with_paths = o.with_paths != 0;
-    SVG_CUDA(cudaMalloc(&g->st_windows, sizeof(int32_t) * (size_t)nv * 3));
+    g->st_windows = dev_alloc_n<int32_t>((size_t)nv * 3);
     g->st_maxq = g->st_windows + nv;
     g->st_flags = g->st_maxq + nv;
     SVG_CUDA(cudaMemsetAsync(g->st_windows, 0, sizeof(int32_t) * (size_t)nv * 3, st));
-    SVG_CUDA(cudaMalloc(&g->off, sizeof(int64_t) * ((size_t)nv + 1)));
+    g->off = dev_alloc_n<int64_t>((size_t)nv + 1);
 
     PhaseOut O{};
     O.order = d_order;
@@ -765,9 +769,9 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     SVG_CUDA(cudaMemcpyAsync(&nnz, g->off + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     SVG_CUDA(cudaStreamSynchronize(st));
     g->nnz = nnz;
-    SVG_CUDA(cudaMalloc(&g->adj, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
-    SVG_CUDA(cudaMalloc(&g->dist, sizeof(double) * (size_t)std::max<int64_t>(nnz, 1)));
-    if (g->with_paths) SVG_CUDA(cudaMalloc(&g->paths, sizeof(PathEnd) * (size_t)std::max<int64_t>(nnz, 1)));
+    g->adj = dev_alloc_n<int32_t>((size_t)std::max<int64_t>(nnz, 1));
+    g->dist = dev_alloc_n<double>((size_t)std::max<int64_t>(nnz, 1));
+    if (g->with_paths) g->paths = dev_alloc(sizeof(PathEnd) * (size_t)std::max<int64_t>(nnz, 1));
     SVG_CUDA(cudaEventRecord(ev[2], st));
 
     if (plain) {

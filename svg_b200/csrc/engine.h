@@ -33,6 +33,16 @@ struct SvgError {
 // The library's CUDA stream and events (one device: the current one at first use).
 cudaStream_t lib_stream();
 
+// Device memory through a caching pool: freed blocks are kept by size and
+// handed out again, so repeated builds and query batches do not pay for
+// cudaMalloc/cudaFree of gigabyte buffers.  dev_free waits for the library
+// stream before a block can be reused.  A failing cudaMalloc releases the
+// cached blocks and retries once.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+size_t dev_trim();  // release every cached block; returns the bytes released
+template <class T> T* dev_alloc_n(size_t n) { return static_cast<T*>(dev_alloc(n * sizeof(T))); }
+
 // Growable device buffer, reused across calls.
 struct DevBuf {
     void* p = nullptr;

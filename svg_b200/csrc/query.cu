@@ -343,13 +343,13 @@ int prepare(svg_graph* g, int want, QParams& P) {
     QState& Q = qstate(g);
     if (Q.delta == 0.0) {
         double* d_sum = nullptr;
-        SVG_CUDA(cudaMalloc(&d_sum, sizeof(double)));
+        d_sum = dev_alloc_n<double>(1);
         SVG_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), st));
         if (g->nnz > 0) k_mean_weight<<<256, 256, 0, st>>>(g->dist, g->nnz, d_sum);
         double sum = 0.0;
         SVG_CUDA(cudaMemcpyAsync(&sum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, st));
         SVG_CUDA(cudaStreamSynchronize(st));
-        cudaFree(d_sum);
+        dev_free(d_sum);
         double mean = g->nnz > 0 ? sum / (double)g->nnz : 1.0;
         Q.delta = mean > 0.0 ? mean : 1.0;
     }
