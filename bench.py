@@ -67,22 +67,29 @@ def init_dist(ws):
     return dist
 
 
-def max_over_ranks(dist, x: float) -> float:
+def _reduce(dist, x: float, op: str, device: str) -> float:
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
 
-def sum_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+def max_over_ranks(dist, x: float, device: str = "cuda") -> float:
+    """Device time of a multi-rank step: the slowest rank's."""
+    return _reduce(dist, x, "max", device)
+
+
+def sum_over_ranks(dist, x: float, device: str = "cuda") -> float:
+    """Work of a multi-rank step: every rank's replica counts."""
+    return _reduce(dist, x, "sum", device)
+
+
+def replica_value(dist, edges_this_rank: float, ms_this_rank: float, device: str = "cuda") -> float:
+    """Whole-job throughput of N replicas: all ranks' edges over the max time."""
+    ms = max_over_ranks(dist, ms_this_rank, device)
+    return sum_over_ranks(dist, edges_this_rank, device) / (ms / 1e3)
 
 
 def barrier(dist):
@@ -293,8 +300,7 @@ def main():
     ck = clocks.stop()
     total_ms = sum(times)
     total_ms_max = max_over_ranks(dist, total_ms)
-    edges_all = sum_over_ranks(dist, float(edges))
-    value = edges_all / (total_ms_max / 1e3)
+    value = replica_value(dist, float(edges), total_ms)
 
     # ---- end to end through the C ABI from host buffers
     posc = np.ascontiguousarray(pos.reshape(-1))
@@ -323,7 +329,7 @@ def main():
         s2.FreeSVGStructure()
         m2.clear()
     e2e_max = max_over_ranks(dist, sum(e2e_ms))
-    e2e_val = sum_over_ranks(dist, float(e2e_edges)) / (e2e_max / 1e3)
+    e2e_val = replica_value(dist, float(e2e_edges), sum(e2e_ms))
 
     out = None
     if rank == 0:
