@@ -204,6 +204,70 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
 svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t source_begin, int32_t source_end,
                                  int32_t* d_tails, int32_t* d_adj, double* d_dist, void* stream);
 
+/* ---------------------------------------------------------------- serving
+ *
+ * A serving loop with no counterpart in the reference (which answers one
+ * query at a time on the host, SVG.cu:241-413).  SVGs stay resident on the
+ * device; a worker thread batches arriving SSSD and MSAD requests per graph
+ * (the oldest pending request plus every other one of the same kind and
+ * graph that fits) and launches each batch on one of `lanes` CUDA streams,
+ * so batches - and a build running on a builder thread - overlap on the GPU;
+ * requests arriving meanwhile join the next batch as soon as a lane frees.
+ * Builds are admitted under `hbm_budget`, evicting least-recently-used idle
+ * graphs the server built itself; a query for an evicted graph triggers its
+ * rebuild and waits for it.  Results are identical to the synchronous batch
+ * calls above. */
+typedef struct svg_server svg_server;
+
+typedef struct svg_server_opts {
+    int64_t hbm_budget;         /* device bytes for resident graphs, query scratch, staging and builds */
+    int32_t lanes;              /* concurrent batches (CUDA streams) */
+    int32_t max_batch;          /* requests per batch */
+    int32_t slots_per_lane;     /* query blocks per batch (one query each at a time) */
+    int32_t pad_;
+    int64_t staging_in_bytes;   /* per lane: request inputs (pinned host + device) */
+    int64_t staging_out_bytes;  /* per lane: results (an MSAD result is 12 bytes per vertex) */
+} svg_server_opts;
+
+typedef struct svg_server_result {
+    int64_t ticket;
+    int32_t status;             /* svg_status of the request */
+    int32_t kind;               /* 0 SSSD, 1 MSAD, 2 build */
+    int32_t graph_id;
+    int32_t n;                  /* MSAD: number of vertices in the result */
+    double latency_ms;          /* submit -> result on the host */
+    double dist;                /* SSSD distance (DBL_MAX if unreachable) */
+} svg_server_result;
+
+typedef struct svg_server_stats_t {
+    int64_t pending;
+    int64_t batches;
+    int64_t batched_requests;
+    int64_t resident_bytes;
+    int64_t evictions;
+    int64_t rebuilds;
+    int64_t resident_graphs;
+} svg_server_stats_t;
+
+void svg_server_opts_default(svg_server_opts* o);
+svg_status svg_server_create(const svg_server_opts* opts, svg_server** out);
+void svg_server_free(svg_server* s);
+/* Serve an already built graph (owned by the caller, never evicted). */
+svg_status svg_server_add_graph(svg_server* s, svg_graph* g, int32_t* graph_id);
+/* Build (asynchronously) and serve the SVG of mesh m; graph_id is usable at once. */
+svg_status svg_server_submit_build(svg_server* s, svg_mesh* m, const svg_build_opts* opts, int32_t* graph_id,
+                                   int64_t* ticket);
+svg_status svg_server_submit_sssd(svg_server* s, int32_t graph_id, int32_t src, int32_t dst, int64_t* ticket);
+svg_status svg_server_submit_msad(svg_server* s, int32_t graph_id, int32_t n, const int32_t* srcs,
+                                  const double* weights, int64_t* ticket);
+/* Wait for one request (timeout_s < 0: no limit). */
+svg_status svg_server_wait(svg_server* s, int64_t ticket, double timeout_s, svg_server_result* res);
+/* Completed requests not yet taken (up to max). */
+svg_status svg_server_poll(svg_server* s, int32_t max, svg_server_result* res, int32_t* n);
+/* Copy an MSAD result (dists[n], src_ids[n], either may be NULL) and release the request. */
+svg_status svg_server_take(svg_server* s, int64_t ticket, double* dists, int32_t* src_ids);
+svg_status svg_server_stats(svg_server* s, svg_server_stats_t* st);
+
 /* Device memory freed by the library (graphs, build scratch, query buffers)
  * is cached for reuse; this returns all cached blocks to CUDA and reports how
  * many bytes it released.  No counterpart in the reference (it cudaMallocs

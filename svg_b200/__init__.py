@@ -24,7 +24,7 @@ import os
 import numpy as np
 
 __all__ = ["Mesh", "SVG", "BuildOptions", "SvgError", "lib", "NODE_DTYPE", "LIB_PATH",
-           "MODE_BATCHED", "MODE_PLAIN"]
+           "MODE_BATCHED", "MODE_PLAIN", "Server", "ServerOptions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("SVG_B200_LIB") or os.path.join(HERE, "libsvg_b200.so")
@@ -72,6 +72,23 @@ class BuildStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget", C.c_int64), ("lanes", C.c_int32), ("max_batch", C.c_int32),
+                ("slots_per_lane", C.c_int32), ("pad", C.c_int32), ("staging_in_bytes", C.c_int64),
+                ("staging_out_bytes", C.c_int64)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("ticket", C.c_int64), ("status", C.c_int32), ("kind", C.c_int32), ("graph_id", C.c_int32),
+                ("n", C.c_int32), ("latency_ms", C.c_double), ("dist", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("pending", C.c_int64), ("batches", C.c_int64), ("batched_requests", C.c_int64),
+                ("resident_bytes", C.c_int64), ("evictions", C.c_int64), ("rebuilds", C.c_int64),
+                ("resident_graphs", C.c_int64)]
+
+
 _P = C.c_void_p
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
@@ -85,6 +102,9 @@ EXPORTS = [
     "svg_graph_copy_nodes", "svg_graph_device_csr", "svg_graph_save", "svg_graph_load", "svg_sssd_batch",
     "svg_msad_batch", "svg_sssd_batch_device", "svg_msad_batch_device", "svg_timer_mark",
     "svg_build_rows_static", "svg_trim_device_cache",
+    "svg_server_opts_default", "svg_server_create", "svg_server_free", "svg_server_add_graph",
+    "svg_server_submit_build", "svg_server_submit_sssd", "svg_server_submit_msad", "svg_server_wait",
+    "svg_server_poll", "svg_server_take", "svg_server_stats",
 ]
 
 _lib = None
@@ -127,6 +147,19 @@ def lib() -> C.CDLL:
     L.svg_timer_mark.argtypes = [C.POINTER(C.c_double)]
     L.svg_build_rows_static.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P]
     L.svg_trim_device_cache.restype = C.c_size_t
+    L.svg_server_opts_default.argtypes = [C.POINTER(ServerOptions)]
+    L.svg_server_opts_default.restype = None
+    L.svg_server_create.argtypes = [C.POINTER(ServerOptions), C.POINTER(_P)]
+    L.svg_server_free.argtypes = [_P]
+    L.svg_server_free.restype = None
+    L.svg_server_add_graph.argtypes = [_P, _P, C.POINTER(C.c_int32)]
+    L.svg_server_submit_build.argtypes = [_P, _P, C.POINTER(BuildOptions), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    L.svg_server_submit_sssd.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]
+    L.svg_server_submit_msad.argtypes = [_P, C.c_int32, C.c_int32, _P, _P, C.POINTER(C.c_int64)]
+    L.svg_server_wait.argtypes = [_P, C.c_int64, C.c_double, C.POINTER(ServerResult)]
+    L.svg_server_poll.argtypes = [_P, C.c_int32, _P, C.POINTER(C.c_int32)]
+    L.svg_server_take.argtypes = [_P, C.c_int64, _P, _P]
+    L.svg_server_stats.argtypes = [_P, C.POINTER(ServerStats)]
     _lib = L
     return L
 
@@ -314,3 +347,84 @@ class SVG:
     def SolveMSAD(self, sources, sourceWeights):
         d, s = self.msad_batch([np.asarray(sources)], [np.asarray(sourceWeights, np.float64)])
         return d[0], s[0]
+
+
+class Server:
+    """Serving loop over resident SVGs (svg_server_* in include/svg_b200.h):
+    continuous batching of SSSD / MSAD requests on several CUDA streams,
+    builds admitted under a device-memory budget with eviction and rebuild."""
+
+    def __init__(self, **opts):
+        self.opts = ServerOptions()
+        lib().svg_server_opts_default(C.byref(self.opts))
+        for k, v in opts.items():
+            setattr(self.opts, k, v)
+        h = _P()
+        _check(lib().svg_server_create(C.byref(self.opts), C.byref(h)))
+        self._h = h
+        self._keep = []   # meshes/graphs the server refers to stay alive with it
+
+    def close(self):
+        if self._h:
+            lib().svg_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_graph(self, svg: "SVG") -> int:
+        gid = C.c_int32()
+        _check(lib().svg_server_add_graph(self._h, svg._g, C.byref(gid)))
+        self._keep.append(svg)
+        return gid.value
+
+    def submit_build(self, mesh: Mesh, K: int, **kw):
+        o = BuildOptions()
+        lib().svg_build_opts_default(C.byref(o))
+        o.K = K
+        for k, v in kw.items():
+            setattr(o, k, v)
+        gid, t = C.c_int32(), C.c_int64()
+        _check(lib().svg_server_submit_build(self._h, mesh._h, C.byref(o), C.byref(gid), C.byref(t)))
+        self._keep.append(mesh)
+        return gid.value, t.value
+
+    def submit_sssd(self, gid: int, s: int, t: int) -> int:
+        tk = C.c_int64()
+        _check(lib().svg_server_submit_sssd(self._h, gid, int(s), int(t), C.byref(tk)))
+        return tk.value
+
+    def submit_msad(self, gid: int, srcs, weights=None) -> int:
+        srcs = np.ascontiguousarray(srcs, np.int32)
+        w = np.zeros(len(srcs)) if weights is None else np.ascontiguousarray(weights, np.float64)
+        tk = C.c_int64()
+        _check(lib().svg_server_submit_msad(self._h, gid, len(srcs), srcs.ctypes.data_as(_P), w.ctypes.data_as(_P),
+                                            C.byref(tk)))
+        return tk.value
+
+    def wait(self, ticket: int, timeout: float = 600.0) -> dict:
+        r = ServerResult()
+        _check(lib().svg_server_wait(self._h, ticket, timeout, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in r._fields_}
+
+    def take(self, ticket: int, nv: int = 0):
+        """Release a finished request; for MSAD return (dists, src_ids) of length nv."""
+        d = np.zeros(max(nv, 1))
+        s = np.zeros(max(nv, 1), np.int32)
+        _check(lib().svg_server_take(self._h, ticket, d.ctypes.data_as(_P) if nv else None,
+                                     s.ctypes.data_as(_P) if nv else None))
+        return (d[:nv], s[:nv]) if nv else None
+
+    def poll(self, max_n: int = 4096) -> list:
+        arr = (ServerResult * max_n)()
+        n = C.c_int32()
+        _check(lib().svg_server_poll(self._h, max_n, C.cast(arr, _P), C.byref(n)))
+        return [{k: getattr(arr[i], k) for k, _ in ServerResult._fields_} for i in range(n.value)]
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().svg_server_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}

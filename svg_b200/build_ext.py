@@ -19,7 +19,7 @@ OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsvg_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU_SOURCES = ["api.cu", "build.cu", "query.cu"]
+CU_SOURCES = ["api.cu", "build.cu", "query.cu", "serve.cu"]
 CPP_SOURCES = ["mesh.cpp"]
 HEADERS = ["svg_internal.h", "engine.h", "ich.cuh"]
 

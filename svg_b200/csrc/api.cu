@@ -160,7 +160,8 @@ void free_graph_device(svg_graph* g) {
     g->dist = nullptr;
     g->paths = nullptr;
     g->st_windows = g->st_maxq = g->st_flags = nullptr;
-    g->qbuf.release();
+    if (g->qdefault) qctx_free(g->qdefault);
+    g->qdefault = nullptr;
 }
 
 }  // namespace svgb

@@ -75,6 +75,8 @@ struct svg_mesh {
     std::vector<int32_t> cost;
 };
 
+struct svg_qctx;
+
 struct svg_graph {
     svg_mesh* mesh = nullptr;
     int32_t K = 0;
@@ -89,8 +91,21 @@ struct svg_graph {
     int32_t* st_maxq = nullptr;
     int32_t* st_flags = nullptr;
     svg_build_stats stats{};
-    // query scratch
-    svgb::DevBuf qbuf;
+    // queries: near-far bucket width (mean edge length) and the context of
+    // the synchronous batch entry points
+    double delta = 0.0;
+    svg_qctx* qdefault = nullptr;
+};
+
+// Scratch of `slots` concurrent queries on one graph (see query.cu).
+struct svg_qctx {
+    svg_graph* g = nullptr;
+    int slots = 0;
+    size_t slot_bytes = 0;
+    int64_t list_cap = 0;
+    svgb::DevBuf buf;
+    uint32_t* stamps = nullptr;
+    int32_t* head = nullptr;
 };
 
 namespace svgb {
@@ -100,4 +115,10 @@ void free_graph_device(svg_graph* g);
 svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist);
 svg_status run_msad(svg_graph* g, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w,
                     double* d_dist, int32_t* d_src_id, int64_t total_srcs);
+double graph_delta(svg_graph* g, cudaStream_t st);
+svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st);
+void qctx_free(svg_qctx* c);
+void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist, cudaStream_t st);
+void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w, double* d_dist,
+               int32_t* d_src_id, cudaStream_t st);
 }  // namespace svgb

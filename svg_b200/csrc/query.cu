@@ -320,87 +320,125 @@ __global__ void k_fill(unsigned long long* p, size_t n, unsigned long long v) {
         p[i] = v;
 }
 
-struct QState {
-    double delta = 0.0;
-    int slots = 0;          // slots initialised in g->qbuf
-    size_t slot_bytes = 0;
-};
-
-QState& qstate(svg_graph* g) {
-    static std::vector<std::pair<svg_graph*, QState>> tab;
-    for (auto& p : tab)
-        if (p.first == g) return p.second;
-    tab.emplace_back(g, QState{});
-    return tab.back().second;
-}
-
 size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 
-// Prepare per-block scratch for up to `want` concurrent query slots; returns
-// the slot count (= grid size).
-int prepare(svg_graph* g, int want, QParams& P) {
-    cudaStream_t st = lib_stream();
-    QState& Q = qstate(g);
-    if (Q.delta == 0.0) {
-        double* d_sum = nullptr;
-        d_sum = dev_alloc_n<double>(1);
-        SVG_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), st));
-        if (g->nnz > 0) k_mean_weight<<<256, 256, 0, st>>>(g->dist, g->nnz, d_sum);
-        double sum = 0.0;
-        SVG_CUDA(cudaMemcpyAsync(&sum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, st));
-        SVG_CUDA(cudaStreamSynchronize(st));
-        dev_free(d_sum);
-        double mean = g->nnz > 0 ? sum / (double)g->nnz : 1.0;
-        Q.delta = mean > 0.0 ? mean : 1.0;
+}  // namespace
+
+// Bucket width of the near-far search: the mean SVG edge length, computed once per graph.
+double graph_delta(svg_graph* g, cudaStream_t st) {
+    if (g->delta > 0.0) return g->delta;
+    double* d_sum = dev_alloc_n<double>(1);
+    SVG_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), st));
+    if (g->nnz > 0) k_mean_weight<<<256, 256, 0, st>>>(g->dist, g->nnz, d_sum);
+    double sum = 0.0;
+    SVG_CUDA(cudaMemcpyAsync(&sum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    dev_free(d_sum);
+    double mean = g->nnz > 0 ? sum / (double)g->nnz : 1.0;
+    g->delta = mean > 0.0 ? mean : 1.0;
+    return g->delta;
+}
+
+// Query scratch for `slots` concurrent queries of one graph: per slot the SSSD
+// distances (kept at +inf between queries), the MSAD {dist, src} pairs, the
+// stamp arrays and the frontier lists; one launch at a time may use it.
+svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st) {
+    graph_delta(g, st);
+    svg_qctx* c = new svg_qctx();
+    c->g = g;
+    c->slots = std::max(1, slots);
+    const size_t V = (size_t)g->nv;
+    c->list_cap = 2 * (int64_t)V + 64;
+    c->slot_bytes = al256(8 * V) + al256(16 * V) + 4 * al256(4 * V) + 2 * al256(4 * (size_t)c->list_cap) + al256(4 * V);
+    const size_t body = al256((size_t)c->slots * c->slot_bytes);
+    const size_t need = body + al256(sizeof(uint32_t) * (size_t)c->slots) + 256;
+    try {
+        c->buf.reserve(need);
+    } catch (...) {
+        delete c;
+        throw;
     }
-    int dev = 0;
-    SVG_CUDA(cudaGetDevice(&dev));
-    int sms = 0;
-    SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    int slots = std::max(1, std::min(want, sms * 2));
-    size_t V = (size_t)g->nv;
-    int64_t list_cap = 2 * (int64_t)V + 64;
-    size_t slot_bytes = al256(8 * V) + al256(16 * V) + 4 * al256(4 * V) + 2 * al256(4 * (size_t)list_cap) + al256(4 * V);
-    if (Q.slots < slots || Q.slot_bytes != slot_bytes) {
-        int ns = std::max(slots, Q.slots);
-        size_t need = al256((size_t)ns * slot_bytes) + al256(sizeof(uint32_t) * (size_t)ns) + 256;
-        g->qbuf.reserve(need);
-        SVG_CUDA(cudaMemsetAsync(g->qbuf.p, 0, need, st));  // stamps and flags start at 0
-        for (int sl = 0; sl < ns; ++sl)  // SSSD distances start at +inf
-            k_fill<<<64, 256, 0, st>>>(reinterpret_cast<unsigned long long*>(g->qbuf.as<char>() + (size_t)sl * slot_bytes),
-                                      V, kInfBits);
-        SVG_CUDA(cudaGetLastError());
-        Q.slots = ns;
-        Q.slot_bytes = slot_bytes;
-    }
-    char* base = g->qbuf.as<char>();
-    P.scratch = base;
-    P.slot_bytes = slot_bytes;
-    P.slot_stamp = reinterpret_cast<uint32_t*>(base + al256((size_t)Q.slots * slot_bytes));
-    P.head = reinterpret_cast<int32_t*>(base + al256((size_t)Q.slots * slot_bytes) + al256(sizeof(uint32_t) * (size_t)Q.slots));
-    P.list_cap = list_cap;
+    char* base = c->buf.as<char>();
+    c->stamps = reinterpret_cast<uint32_t*>(base + body);
+    c->head = reinterpret_cast<int32_t*>(base + body + al256(sizeof(uint32_t) * (size_t)c->slots));
+    SVG_CUDA(cudaMemsetAsync(base, 0, need, st));  // stamps and flags start at 0
+    for (int sl = 0; sl < c->slots; ++sl)          // SSSD distances start at +inf
+        k_fill<<<64, 256, 0, st>>>(reinterpret_cast<unsigned long long*>(base + (size_t)sl * c->slot_bytes), V,
+                                  kInfBits);
+    SVG_CUDA(cudaGetLastError());
+    SVG_CUDA(cudaStreamSynchronize(st));
+    return c;
+}
+
+void qctx_free(svg_qctx* c) { delete c; }
+
+namespace {
+void fill_params(svg_qctx* c, QParams& P) {
+    svg_graph* g = c->g;
+    P.scratch = c->buf.as<char>();
+    P.slot_bytes = c->slot_bytes;
+    P.slot_stamp = c->stamps;
+    P.head = c->head;
+    P.list_cap = c->list_cap;
     P.off = g->off;
     P.adj = g->adj;
     P.w = g->dist;
     P.pos = g->mesh->d.pos;
     P.nv = g->nv;
-    P.delta = Q.delta;
+    P.delta = g->delta;
+}
+}  // namespace
+
+void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist, cudaStream_t st) {
+    if (n <= 0) return;
+    QParams P{};
+    fill_params(c, P);
+    P.n = n;
+    P.s = d_s;
+    P.t = d_t;
+    P.out = d_dist;
     SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
-    return slots;
+    k_query<true, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
+    SVG_CUDA(cudaGetLastError());
+}
+
+void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w, double* d_dist,
+               int32_t* d_src_id, cudaStream_t st) {
+    if (n <= 0) return;
+    QParams P{};
+    fill_params(c, P);
+    P.n = n;
+    P.set_off = d_off;
+    P.srcs = d_src;
+    P.weights = d_w;
+    P.out_dist = d_dist;
+    P.out_src = d_src_id;
+    SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
+    if (d_src_id)
+        k_query<false, true><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
+    else
+        k_query<false, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
+    SVG_CUDA(cudaGetLastError());
+}
+
+namespace {
+// The graph's own context for the synchronous batch entry points: two query
+// blocks per SM.
+svg_qctx* default_ctx(svg_graph* g) {
+    if (!g->qdefault) {
+        int dev = 0, sms = 0;
+        SVG_CUDA(cudaGetDevice(&dev));
+        SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        g->qdefault = qctx_create(g, 2 * sms, lib_stream());
+    }
+    return g->qdefault;
 }
 
 }  // namespace
 
 svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist) {
     if (n == 0) return SVG_OK;
-    QParams P{};
-    int slots = prepare(g, n, P);
-    P.n = n;
-    P.s = d_s;
-    P.t = d_t;
-    P.out = d_dist;
-    k_query<true, false><<<slots, kQThreads, 0, lib_stream()>>>(P);
-    SVG_CUDA(cudaGetLastError());
+    qctx_sssd(default_ctx(g), n, d_s, d_t, d_dist, lib_stream());
     return SVG_OK;
 }
 
@@ -408,19 +446,7 @@ svg_status run_msad(svg_graph* g, int32_t n, const int64_t* d_off, const int32_t
                     double* d_dist, int32_t* d_src_id, int64_t total_srcs) {
     (void)total_srcs;
     if (n == 0) return SVG_OK;
-    QParams P{};
-    int slots = prepare(g, n, P);
-    P.n = n;
-    P.set_off = d_off;
-    P.srcs = d_src;
-    P.weights = d_w;
-    P.out_dist = d_dist;
-    P.out_src = d_src_id;
-    if (d_src_id)
-        k_query<false, true><<<slots, kQThreads, 0, lib_stream()>>>(P);
-    else
-        k_query<false, false><<<slots, kQThreads, 0, lib_stream()>>>(P);
-    SVG_CUDA(cudaGetLastError());
+    qctx_msad(default_ctx(g), n, d_off, d_src, d_w, d_dist, d_src_id, lib_stream());
     return SVG_OK;
 }
 
