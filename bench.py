@@ -235,6 +235,311 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- other configurations
+# `--workload large` (750K-vertex torus builds) and `--workload serve` (serving
+# loop on its K=100 graph) print their own JSON line; the default workload is
+# the build benchmark above.
+
+LARGE = dict(mesh="torus_value_noise", R=1.0, r=0.4, grid="1000x750", vertices=750000, seed=2)
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def _gpu_setup():
+    import torch
+    ws, rank, local = dist_env()
+    if ws != 1:
+        raise SystemExit("this workload runs on one GPU")
+    torch.cuda.set_device(local)
+    from svg_b200.build_ext import build as build_lib
+    build_lib()
+    return torch
+
+
+def work_histogram(windows: np.ndarray) -> dict:
+    """Per-source propagated windows: log2 buckets and spread."""
+    w = np.asarray(windows, np.int64)
+    w = w[w > 0]
+    if len(w) == 0:
+        return {}
+    b = np.floor(np.log2(w)).astype(np.int64)
+    cnt = np.bincount(b)
+    srt = np.sort(w)[::-1]
+    top = max(1, len(w) // 100)
+    return {"log2_buckets": {f"[2^{i},2^{i + 1})": int(c) for i, c in enumerate(cnt) if c},
+            "min": int(w.min()), "median": float(np.median(w)), "p99": _pct(w, 99), "max": int(w.max()),
+            "max_over_median": float(w.max() / np.median(w)),
+            "top1pct_share": float(srt[:top].sum() / w.sum())}
+
+
+def run_large(args):
+    """750K-vertex torus (5-octave value noise, seed 2) built at each K with the
+    batched kernel under a stated build-scratch budget: time, edges/s, peak
+    device memory, per-source work histogram; the plain form on a leading
+    slice of sources, extrapolated to the whole mesh (labelled)."""
+    torch = _gpu_setup()
+    import svg_b200
+    from svg_b200 import SVG, Mesh, MODE_PLAIN, meshgen
+    L = svg_b200.lib()
+    t0 = time.perf_counter()
+    pos, faces = meshgen.config_mesh(2, args.scale)
+    mesh = Mesh.from_arrays(pos, faces)
+    mesh.copyToGPU()
+    mesh_s = time.perf_counter() - t0
+    V = mesh.vertNum
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    budget = int(args.hbm_budget_gb * (1 << 30))
+
+    def mark():
+        x = C.c_double()
+        L.svg_timer_mark(C.byref(x))
+        return x.value
+
+    out = []
+    for K in [int(k) for k in args.K.split(",")]:
+        svg = SVG()
+        svg.AssignMesh(mesh)
+        svg.SetParameters(K)
+        for _ in range(args.warmup):   # the first build also records per-source costs (heavy-first order)
+            svg.ConstructSVG(hbm_budget=budget)
+        svg.FreeSVGStructure()
+        svg_b200.device_memory(reset_peak=True)
+        times, st = [], None
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            mark()
+            st = svg.ConstructSVG(hbm_budget=budget)
+            times.append(mark())
+        mem = svg_b200.device_memory()
+        w, q, f = svg.source_stats()
+        row = {"K": K, "build_s": statistics.mean(times) / 1e3, "build_s_all": [t / 1e3 for t in times],
+               "edges": st["edges"], "edges_per_s": st["edges"] / (statistics.mean(times) / 1e3),
+               "windows": st["windows"], "kernel_ms_ich": st["ms_ich"], "kernel_ms_emit": st["ms_emit"],
+               "peak_device_bytes": mem["peak"], "scratch_bytes": st["scratch_bytes"],
+               "hbm_budget_bytes": budget, "work_histogram": work_histogram(w),
+               "flags": {k: st[k] for k in ("queue_drop_sources", "ref_overflow_sources", "watchdog_sources",
+                                            "undefined_sources", "retried_sources")}}
+        svg.FreeSVGStructure()
+        if args.plain_frac > 0:
+            n = max(1, int(V * args.plain_frac))
+            p = SVG()
+            p.AssignMesh(mesh)
+            p.SetParameters(K)
+            flush.zero_()
+            torch.cuda.synchronize()
+            mark()
+            stp = p.ConstructSVG(mode=MODE_PLAIN, source_begin=0, source_end=n)
+            ms = mark()
+            p.FreeSVGStructure()
+            full = ms / 1e3 * V / n
+            row["plain"] = {"sources": n, "build_s": ms / 1e3, "edges": stp["edges"],
+                            "est_full_build_s": full, "speedup_batched_vs_plain_est": full / row["build_s"],
+                            "note": f"plain form (64x128 grid, one source per thread) on sources [0,{n}) "
+                                    f"of {V}, time scaled by {V}/{n}"}
+        out.append(row)
+        log(json.dumps(row))
+    line = {"metric": "svg_build_edges_per_s", "value": out[-1]["edges_per_s"], "unit": "edges/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(LARGE, workload=f"svg_build_torus_1000x750_value_noise_K{args.K.replace(',', '_')}",
+                           vertices=V, scale=args.scale, l2="flushed between steps (256 MiB write)"),
+            "mesh_host_build_and_upload_s": mesh_s, "per_K": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def make_stream(V: int, rate: float, duration: float, seed: int = 3):
+    """Poisson arrivals at `rate`/s for `duration` s: 70 % SSSD on uniform
+    random pairs, 30 % MSAD with log-uniform set sizes in [1, 1000] of uniform
+    random vertices (duplicates removed), weights 0."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, int(rate * duration * 1.3) + 64)
+    arr = np.cumsum(gaps)
+    arr = arr[arr < duration]
+    n = len(arr)
+    is_sssd = rng.random(n) < 0.7
+    reqs = []
+    for i in range(n):
+        if is_sssd[i]:
+            a, b = rng.integers(0, V, 2)
+            reqs.append((float(arr[i]), 0, int(a), int(b)))
+        else:
+            k = int(np.clip(np.rint(np.exp(rng.uniform(0.0, np.log(1000.0)))), 1, 1000))
+            reqs.append((float(arr[i]), 1, np.unique(rng.integers(0, V, k)).astype(np.int32), None))
+    return reqs
+
+
+def run_serve(args):
+    """Serving on the resident K=100 SVG of the 750K-vertex torus: a Poisson
+    stream through the serving loop (continuous batching), then the plain
+    form (one query per launch, synchronous) on the stream's first requests."""
+    import threading
+    torch = _gpu_setup()
+    import svg_b200
+    from svg_b200 import SVG, Mesh, Server, meshgen
+    pos, faces = meshgen.config_mesh(2, args.scale)
+    mesh = Mesh.from_arrays(pos, faces)
+    mesh.copyToGPU()
+    V = mesh.vertNum
+    svg = SVG()
+    svg.AssignMesh(mesh)
+    svg.SetParameters(100)
+    bst = svg.ConstructSVG()
+    reqs = make_stream(V, args.rate, args.duration)
+    n = len(reqs)
+    log(f"serve: V={V} edges={bst['edges']} requests={n}")
+
+    srv = Server(lanes=args.lanes, max_batch=args.max_batch, max_batch_msad=args.max_batch_msad,
+                 slots_per_lane=args.slots, cluster=args.cluster, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
+                 staging_in_bytes=16 << 20, staging_out_bytes=int(args.staging_out_mb) << 20)
+    gid = srv.add_graph(svg)
+    # warm-up: a few requests of each kind
+    wt = [srv.submit_sssd(gid, i, V - 1 - i) for i in range(64)]
+    wt += [srv.submit_msad(gid, np.array([i], np.int32), out=(None, None)) for i in range(8)]
+    for t in wt:
+        srv.wait(t, 600.0)
+        srv.take(t)
+
+    RING = args.ring
+    ring_d = [np.zeros(V) for _ in range(RING)]
+    ring_s = [np.zeros(V, np.int32) for _ in range(RING)]
+    ring_free = threading.Semaphore(RING)
+    ring_next = [0]
+    slot_of = {}
+    kind_of = {}
+    lat = {0: [], 1: []}
+    done_n = [0]
+    t_done = [0.0]
+    samples = {}
+    want = {i for i in range(n) if i < 400}
+    ticket_req = {}
+    lag = []
+    lock = threading.Lock()
+    finished = threading.Event()
+
+    def collector():
+        while done_n[0] < n:
+            res = srv.poll(4096)
+            if not res:
+                time.sleep(0.0002)
+                continue
+            for r in res:
+                t = r["ticket"]
+                with lock:
+                    i = ticket_req.get(t)
+                if i is None:       # submitted but not yet registered: next poll
+                    continue
+                if r["status"] != 0:
+                    raise RuntimeError(f"request {i} failed with status {r['status']}")
+                k = kind_of[t]
+                lat[k].append(r["latency_ms"])
+                if i in want:
+                    samples[i] = r["dist"] if k == 0 else ring_d[slot_of[t]].copy()
+                srv.take(t)
+                if k == 1:
+                    ring_free.release()
+                done_n[0] += 1
+            t_done[0] = time.perf_counter()
+        finished.set()
+
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
+    st0 = srv.stats()
+    t0 = time.perf_counter()
+    for i, (ta, kind, a, b) in enumerate(reqs):
+        target = t0 + ta
+        now = time.perf_counter()
+        if now < target:
+            time.sleep(max(0.0, target - now - 0.0001))
+            while time.perf_counter() < target:
+                pass
+        lag.append((time.perf_counter() - target) * 1e3)
+        if kind == 0:
+            t = srv.submit_sssd(gid, a, b)
+        else:
+            ring_free.acquire()
+            sl = ring_next[0] % RING
+            ring_next[0] += 1
+            t = srv.submit_msad(gid, a, out=(ring_d[sl], ring_s[sl]))
+            slot_of[t] = sl
+        kind_of[t] = kind
+        with lock:
+            ticket_req[t] = i
+    finished.wait(args.duration * 20 + 600)
+    wall = t_done[0] - t0
+    st1 = srv.stats()
+    srv.close()
+
+    # results equal the synchronous batch calls
+    mism = 0
+    for i, v in samples.items():
+        _, kind, a, b = reqs[i]
+        if kind == 0:
+            mism += int(v != svg.sssd_batch(np.array([a], np.int32), np.array([b], np.int32))[0])
+        else:
+            d, _ = svg.msad_batch([a])
+            mism += int(not np.array_equal(v, d[0]))
+
+    # one query per launch, synchronous, on the stream's first requests: the
+    # plain form (one block per query, the reference's one-search-at-a-time
+    # form) and, for the latency floor, the cluster form
+    def one_per_launch(form):
+        svg.set_query_form(form)
+        svg.sssd_batch(np.array([0], np.int32), np.array([1], np.int32))   # query context set-up
+        svg.msad_batch([np.array([0], np.int32)])
+        tms = {0: [], 1: []}
+        tp0 = time.perf_counter()
+        for i, (_, kind, a, b) in enumerate(reqs):
+            if i >= args.plain_requests or time.perf_counter() - tp0 > args.plain_seconds:
+                break
+            t1 = time.perf_counter()
+            if kind == 0:
+                svg.sssd_batch(np.array([a], np.int32), np.array([b], np.int32))
+            else:
+                svg.msad_batch([a])
+            tms[kind].append((time.perf_counter() - t1) * 1e3)
+        return tms
+
+    from svg_b200 import QUERY_CLUSTER, QUERY_PLAIN
+    plain_t = one_per_launch(QUERY_PLAIN)
+    single_t = one_per_launch(QUERY_CLUSTER)
+    allp = plain_t[0] + plain_t[1]
+    plain_qps = len(allp) / (sum(allp) / 1e3) if allp else None
+    alls = single_t[0] + single_t[1]
+    alll = lat[0] + lat[1]
+    qps = n / wall
+    line = {"metric": "serve_qps", "value": qps, "unit": "req/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(LARGE, workload="serve_torus_1000x750_K100_poisson", K=100, vertices=V,
+                           rate_per_s=args.rate, duration_s=args.duration, requests=n, sssd_share=0.7,
+                           msad_set_size="log-uniform [1,1000]", seed=3, lanes=args.lanes,
+                           max_batch=args.max_batch, max_batch_msad=args.max_batch_msad, slots_per_lane=args.slots,
+                           cluster=args.cluster, scale=args.scale),
+            "offered_per_s": n / args.duration, "wall_s": wall,
+            "latency_ms": {"all": {"p50": _pct(alll, 50), "p99": _pct(alll, 99)},
+                           "sssd": {"p50": _pct(lat[0], 50), "p99": _pct(lat[0], 99), "n": len(lat[0])},
+                           "msad": {"p50": _pct(lat[1], 50), "p99": _pct(lat[1], 99), "n": len(lat[1])}},
+            "submit_lag_ms": {"p50": _pct(lag, 50), "p99": _pct(lag, 99)},
+            "batches": st1["batches"] - st0["batches"],
+            "mean_batch": (st1["batched_requests"] - st0["batched_requests"]) / max(1, st1["batches"] - st0["batches"]),
+            "checked_vs_sync": len(samples), "mismatches_vs_sync": mism,
+            "plain": {"requests": len(allp), "qps": plain_qps,
+                      "latency_ms": {"all": {"p50": _pct(allp, 50), "p99": _pct(allp, 99)},
+                                     "sssd": {"p50": _pct(plain_t[0], 50), "p99": _pct(plain_t[0], 99)},
+                                     "msad": {"p50": _pct(plain_t[1], 50), "p99": _pct(plain_t[1], 99)}},
+                      "form": "one query per launch, synchronous, inputs from and result to host"},
+            "one_per_launch_cluster": {"requests": len(alls), "qps": len(alls) / (sum(alls) / 1e3) if alls else None,
+                                       "latency_ms": {"sssd": {"p50": _pct(single_t[0], 50), "p99": _pct(single_t[0], 99)},
+                                                      "msad": {"p50": _pct(single_t[1], 50), "p99": _pct(single_t[1], 99)}}},
+            "qps_vs_plain": (qps / plain_qps) if plain_qps else None,
+            "build": {"edges": bst["edges"], "ms": bst["ms_total"]}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -244,9 +549,29 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="build", choices=["build", "large", "serve"])
+    ap.add_argument("--scale", type=float, default=1.0, help="large/serve: grid scale of the 750K torus")
+    ap.add_argument("--K", default="100,500", help="large: build K values")
+    ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
+    ap.add_argument("--plain-frac", type=float, default=0.02, help="large: share of sources built plain")
+    ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--lanes", type=int, default=0, help="serve: 0 = one lane per resident query cluster")
+    ap.add_argument("--max-batch", type=int, default=4, help="serve: SSSD requests per batch")
+    ap.add_argument("--max-batch-msad", type=int, default=1, help="serve: MSAD requests per batch")
+    ap.add_argument("--slots", type=int, default=0, help="serve: queries a lane serves at once (0 = auto)")
+    ap.add_argument("--cluster", type=int, default=0, help="serve: blocks per query (0 auto, -1 one block)")
+    ap.add_argument("--staging-out-mb", type=int, default=64)
+    ap.add_argument("--ring", type=int, default=256)
+    ap.add_argument("--plain-requests", type=int, default=400)
+    ap.add_argument("--plain-seconds", type=float, default=30.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "large":
+        return run_large(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     ws, rank, local = dist_env()
     import torch

@@ -138,6 +138,14 @@ svg_status svg_graph_source_stats(const svg_graph* g, int32_t* windows, int32_t*
 /* SVG::FreeSVGStructure (SVG.cu:149-155). */
 void svg_graph_free(svg_graph* g);
 
+/* Kernel form of the query calls on this graph.  CLUSTER (default): one query
+ * per thread-block cluster of 8-16 SMs, few queries in flight so that their
+ * state stays in L2.  PLAIN: one query per thread block, the reference's
+ * one-search-at-a-time form (SVG::SolveSSSD / SolveMSAD, SVG.cu:241-413),
+ * kept as the baseline.  Results are the same in both forms. */
+enum { SVG_QUERY_CLUSTER = 0, SVG_QUERY_PLAIN = 1 };
+svg_status svg_graph_set_query_form(svg_graph* g, int32_t form);
+
 /* Vertex count, edge count, K of the build. */
 svg_status svg_graph_counts(const svg_graph* g, int32_t* nv, int64_t* nnz, int32_t* K);
 
@@ -221,12 +229,14 @@ typedef struct svg_server svg_server;
 
 typedef struct svg_server_opts {
     int64_t hbm_budget;         /* device bytes for resident graphs, query scratch, staging and builds */
-    int32_t lanes;              /* concurrent batches (CUDA streams) */
-    int32_t max_batch;          /* requests per batch */
-    int32_t slots_per_lane;     /* query blocks per batch (one query each at a time) */
-    int32_t pad_;
+    int32_t lanes;              /* concurrent batches (CUDA streams); 0: one per resident query cluster */
+    int32_t max_batch;          /* SSSD requests per batch */
+    int32_t slots_per_lane;     /* queries of one batch served at once (0: the GPU's share of the lane) */
+    int32_t cluster;            /* blocks per query: 0 automatic cluster, -1 one block (plain form), 8 or 16 */
     int64_t staging_in_bytes;   /* per lane: request inputs (pinned host + device) */
     int64_t staging_out_bytes;  /* per lane: results (an MSAD result is 12 bytes per vertex) */
+    int32_t max_batch_msad;     /* MSAD requests per batch (each is a whole-graph search) */
+    int32_t pad_;
 } svg_server_opts;
 
 typedef struct svg_server_result {
@@ -260,6 +270,11 @@ svg_status svg_server_submit_build(svg_server* s, svg_mesh* m, const svg_build_o
 svg_status svg_server_submit_sssd(svg_server* s, int32_t graph_id, int32_t src, int32_t dst, int64_t* ticket);
 svg_status svg_server_submit_msad(svg_server* s, int32_t graph_id, int32_t n, const int32_t* srcs,
                                   const double* weights, int64_t* ticket);
+/* As svg_server_submit_msad, with the result written straight into the
+ * caller's host buffers dists[V] and src_ids[V] (either may be NULL to drop
+ * it); they must stay valid until the request is finished. */
+svg_status svg_server_submit_msad_into(svg_server* s, int32_t graph_id, int32_t n, const int32_t* srcs,
+                                       const double* weights, double* dists, int32_t* src_ids, int64_t* ticket);
 /* Wait for one request (timeout_s < 0: no limit). */
 svg_status svg_server_wait(svg_server* s, int64_t ticket, double timeout_s, svg_server_result* res);
 /* Completed requests not yet taken (up to max). */
@@ -273,6 +288,11 @@ svg_status svg_server_stats(svg_server* s, svg_server_stats_t* st);
  * many bytes it released.  No counterpart in the reference (it cudaMallocs
  * and cudaFrees every buffer). */
 size_t svg_trim_device_cache(void);
+
+/* Device bytes the library holds: in use by live objects, the high-water mark
+ * of that since the last reset, and cached for reuse.  reset_peak != 0 sets
+ * the high-water mark to the current use.  No counterpart in the reference. */
+void svg_device_memory(int64_t* in_use, int64_t* peak, int64_t* cached, int32_t reset_peak);
 
 /* Synchronise the library's stream; returns the device time in ms since the
  * previous svg_timer_mark (CUDA events on the library stream). */

@@ -24,11 +24,12 @@ import os
 import numpy as np
 
 __all__ = ["Mesh", "SVG", "BuildOptions", "SvgError", "lib", "NODE_DTYPE", "LIB_PATH",
-           "MODE_BATCHED", "MODE_PLAIN", "Server", "ServerOptions"]
+           "MODE_BATCHED", "MODE_PLAIN", "QUERY_CLUSTER", "QUERY_PLAIN", "Server", "ServerOptions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("SVG_B200_LIB") or os.path.join(HERE, "libsvg_b200.so")
 MODE_BATCHED, MODE_PLAIN = 0, 1
+QUERY_CLUSTER, QUERY_PLAIN = 0, 1
 DBL_MAX = np.finfo(np.float64).max
 
 # svg_node: the reference's SVGNode layout (SVG.cuh:21-27), 40 bytes
@@ -74,8 +75,8 @@ class BuildStats(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget", C.c_int64), ("lanes", C.c_int32), ("max_batch", C.c_int32),
-                ("slots_per_lane", C.c_int32), ("pad", C.c_int32), ("staging_in_bytes", C.c_int64),
-                ("staging_out_bytes", C.c_int64)]
+                ("slots_per_lane", C.c_int32), ("cluster", C.c_int32), ("staging_in_bytes", C.c_int64),
+                ("staging_out_bytes", C.c_int64), ("max_batch_msad", C.c_int32), ("pad", C.c_int32)]
 
 
 class ServerResult(C.Structure):
@@ -104,7 +105,8 @@ EXPORTS = [
     "svg_build_rows_static", "svg_trim_device_cache",
     "svg_server_opts_default", "svg_server_create", "svg_server_free", "svg_server_add_graph",
     "svg_server_submit_build", "svg_server_submit_sssd", "svg_server_submit_msad", "svg_server_wait",
-    "svg_server_poll", "svg_server_take", "svg_server_stats",
+    "svg_server_poll", "svg_server_take", "svg_server_stats", "svg_server_submit_msad_into",
+    "svg_device_memory", "svg_graph_set_query_form",
 ]
 
 _lib = None
@@ -156,6 +158,10 @@ def lib() -> C.CDLL:
     L.svg_server_submit_build.argtypes = [_P, _P, C.POINTER(BuildOptions), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.svg_server_submit_sssd.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]
     L.svg_server_submit_msad.argtypes = [_P, C.c_int32, C.c_int32, _P, _P, C.POINTER(C.c_int64)]
+    L.svg_server_submit_msad_into.argtypes = [_P, C.c_int32, C.c_int32, _P, _P, _P, _P, C.POINTER(C.c_int64)]
+    L.svg_device_memory.argtypes = [C.POINTER(C.c_int64)] * 3 + [C.c_int32]
+    L.svg_device_memory.restype = None
+    L.svg_graph_set_query_form.argtypes = [_P, C.c_int32]
     L.svg_server_wait.argtypes = [_P, C.c_int64, C.c_double, C.POINTER(ServerResult)]
     L.svg_server_poll.argtypes = [_P, C.c_int32, _P, C.POINTER(C.c_int32)]
     L.svg_server_take.argtypes = [_P, C.c_int64, _P, _P]
@@ -316,6 +322,10 @@ class SVG:
         self._g = h
 
     # ---- queries
+    def set_query_form(self, form: int) -> None:
+        """QUERY_CLUSTER (default) or QUERY_PLAIN (one block per query)."""
+        _check(lib().svg_graph_set_query_form(self._g, int(form)))
+
     def sssd_batch(self, s, t) -> np.ndarray:
         s = np.ascontiguousarray(s, np.int32)
         t = np.ascontiguousarray(t, np.int32)
@@ -397,12 +407,23 @@ class Server:
         _check(lib().svg_server_submit_sssd(self._h, gid, int(s), int(t), C.byref(tk)))
         return tk.value
 
-    def submit_msad(self, gid: int, srcs, weights=None) -> int:
+    def submit_msad(self, gid: int, srcs, weights=None, out=None) -> int:
+        """out=(dists, src_ids): float64 / int32 arrays of V entries (either None)
+        that receive the result directly; they must outlive the request."""
         srcs = np.ascontiguousarray(srcs, np.int32)
         w = np.zeros(len(srcs)) if weights is None else np.ascontiguousarray(weights, np.float64)
         tk = C.c_int64()
-        _check(lib().svg_server_submit_msad(self._h, gid, len(srcs), srcs.ctypes.data_as(_P), w.ctypes.data_as(_P),
-                                            C.byref(tk)))
+        if out is None:
+            _check(lib().svg_server_submit_msad(self._h, gid, len(srcs), srcs.ctypes.data_as(_P),
+                                                w.ctypes.data_as(_P), C.byref(tk)))
+        else:
+            d, sid = out
+            assert d is None or (d.dtype == np.float64 and d.flags.c_contiguous)
+            assert sid is None or (sid.dtype == np.int32 and sid.flags.c_contiguous)
+            _check(lib().svg_server_submit_msad_into(self._h, gid, len(srcs), srcs.ctypes.data_as(_P),
+                                                     w.ctypes.data_as(_P),
+                                                     None if d is None else d.ctypes.data_as(_P),
+                                                     None if sid is None else sid.ctypes.data_as(_P), C.byref(tk)))
         return tk.value
 
     def wait(self, ticket: int, timeout: float = 600.0) -> dict:
@@ -428,3 +449,10 @@ class Server:
         st = ServerStats()
         _check(lib().svg_server_stats(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+def device_memory(reset_peak: bool = False) -> dict:
+    """Device bytes held by the library: in use, high-water mark, cached for reuse."""
+    a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+    lib().svg_device_memory(C.byref(a), C.byref(b), C.byref(c), 1 if reset_peak else 0)
+    return {"in_use": a.value, "peak": b.value, "cached": c.value}

@@ -31,6 +31,7 @@ struct Pool {
     std::multimap<size_t, void*> free_blocks;      // size -> block
     std::unordered_map<void*, size_t> live;        // block -> size
     size_t cached = 0;
+    size_t in_use = 0, peak = 0;                   // bytes of live blocks, high-water mark
 };
 Pool& pool() {
     static Pool* P = new Pool();  // never destroyed: blocks may be freed during process exit
@@ -57,6 +58,8 @@ void* dev_alloc(size_t bytes) {
             P.free_blocks.erase(it);
             P.cached -= sz;
             P.live[q] = sz;
+            P.in_use += sz;
+            P.peak = std::max(P.peak, P.in_use);
             return q;
         }
     }
@@ -74,6 +77,8 @@ void* dev_alloc(size_t bytes) {
     }
     std::lock_guard<std::mutex> lk(P.mu);
     P.live[q] = n;
+    P.in_use += n;
+    P.peak = std::max(P.peak, P.in_use);
     return q;
 }
 
@@ -86,7 +91,17 @@ void dev_free(void* q) {
     if (it == P.live.end()) return;
     P.free_blocks.emplace(it->second, q);
     P.cached += it->second;
+    P.in_use -= it->second;
     P.live.erase(it);
+}
+
+void dev_usage(size_t* in_use, size_t* peak, size_t* cached, bool reset_peak) {
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    if (reset_peak) P.peak = P.in_use;
+    if (in_use) *in_use = P.in_use;
+    if (peak) *peak = P.peak;
+    if (cached) *cached = P.cached;
 }
 
 size_t dev_trim() {
@@ -511,6 +526,20 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
     });
 }
 
+svg_status svg_graph_set_query_form(svg_graph* g, int32_t form) {
+    return guarded([&]() -> svg_status {
+        if (!g || (form != SVG_QUERY_CLUSTER && form != SVG_QUERY_PLAIN))
+            throw SvgError{SVG_ERR_ARG, "bad argument"};
+        if (g->qform != form && g->qdefault) {
+            SVG_CUDA(cudaStreamSynchronize(lib_stream()));
+            qctx_free(g->qdefault);
+            g->qdefault = nullptr;
+        }
+        g->qform = form;
+        return SVG_OK;
+    });
+}
+
 svg_status svg_sssd_batch(svg_graph* g, int32_t n, const int32_t* s, const int32_t* t, double* dist) {
     return guarded([&]() -> svg_status {
         if (!g || n < 0 || (n > 0 && (!s || !t || !dist))) throw SvgError{SVG_ERR_ARG, "bad argument"};
@@ -574,6 +603,14 @@ svg_status svg_msad_batch(svg_graph* g, int32_t n, const int64_t* set_offsets, c
 }
 
 size_t svg_trim_device_cache(void) { return dev_trim(); }
+
+void svg_device_memory(int64_t* in_use, int64_t* peak, int64_t* cached, int32_t reset_peak) {
+    size_t a = 0, b = 0, c = 0;
+    dev_usage(&a, &b, &c, reset_peak != 0);
+    if (in_use) *in_use = (int64_t)a;
+    if (peak) *peak = (int64_t)b;
+    if (cached) *cached = (int64_t)c;
+}
 
 svg_status svg_timer_mark(double* ms_since_last) {
     return guarded([&]() -> svg_status {

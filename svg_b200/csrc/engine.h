@@ -41,6 +41,8 @@ cudaStream_t lib_stream();
 void* dev_alloc(size_t bytes);
 void dev_free(void* p);
 size_t dev_trim();  // release every cached block; returns the bytes released
+// bytes of live blocks, their high-water mark, bytes cached for reuse
+void dev_usage(size_t* in_use, size_t* peak, size_t* cached, bool reset_peak);
 template <class T> T* dev_alloc_n(size_t n) { return static_cast<T*>(dev_alloc(n * sizeof(T))); }
 
 // Growable device buffer, reused across calls.
@@ -95,6 +97,7 @@ struct svg_graph {
     // the synchronous batch entry points
     double delta = 0.0;
     svg_qctx* qdefault = nullptr;
+    int32_t qform = SVG_QUERY_CLUSTER;  // kernel form of the synchronous query calls
 };
 
 // Scratch of `slots` concurrent queries on one graph (see query.cu).
@@ -106,6 +109,7 @@ struct svg_qctx {
     svgb::DevBuf buf;
     uint32_t* stamps = nullptr;
     int32_t* head = nullptr;
+    int cluster = 0;  // blocks per query: a cluster of them, or 0 for one block (the plain form)
 };
 
 namespace svgb {
@@ -116,7 +120,10 @@ svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* 
 svg_status run_msad(svg_graph* g, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w,
                     double* d_dist, int32_t* d_src_id, int64_t total_srcs);
 double graph_delta(svg_graph* g, cudaStream_t st);
-svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st);
+svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st, int cluster);
+int query_slots_per_sm();            // plain form: query blocks resident per SM
+int query_cluster_size();            // cluster form: blocks per query
+int query_cluster_slots(int csize);  // cluster form: clusters resident at once
 void qctx_free(svg_qctx* c);
 void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist, cudaStream_t st);
 void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w, double* d_dist,

@@ -19,13 +19,25 @@
 // Per-slot stamp arrays replace clearing: a stamp is never reused.
 #include <cfloat>
 
+#include <cooperative_groups.h>
+
 #include "engine.h"
 
 namespace svgb {
 
 namespace {
 
-constexpr int kQThreads = 512;
+#ifndef SVG_Q_THREADS
+#define SVG_Q_THREADS 512
+#endif
+#ifndef SVG_Q_UNROLL
+#define SVG_Q_UNROLL 4
+#endif
+constexpr int kQThreads = SVG_Q_THREADS;
+// edges per lane whose loads are issued together before any is used: the
+// gather of the head's distance waits on the adjacency load, so issuing
+// several of these chains at once hides most of their latency
+constexpr int kQUnroll = SVG_Q_UNROLL;
 constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;  // +inf
 
 struct alignas(16) DS {
@@ -227,41 +239,66 @@ __global__ void __launch_bounds__(kQThreads) k_query(QParams P) {
                         du = as_d(z.d);
                         su = z.s;
                     }
-                    int64_t e0 = P.off[u], e1 = P.off[u + 1];
-                    for (int64_t e = e0 + lane; e < e1; e += 32) {
-                        int w = P.adj[e];
-                        double nd = du + P.w[e];
-                        bool improved = false, first = false;
-                        if (kSSSD) {
-                            unsigned long long cur = S.dist[w];
-                            if (nd < as_d(cur)) {
-                                unsigned long long old = atomicMin(&S.dist[w], as_b(nd));
-                                improved = nd < as_d(old);
+                    const int64_t e0 = P.off[u], e1 = P.off[u + 1];
+                    for (int64_t eb = e0 + lane; eb < e1; eb += 32 * kQUnroll) {
+                        int wv[kQUnroll];
+                        double nd[kQUnroll];
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            const int64_t e = eb + 32 * j;
+                            wv[j] = e < e1 ? __ldg(&P.adj[e]) : -1;
+                            nd[j] = e < e1 ? du + __ldg(&P.w[e]) : 0.0;
+                        }
+                        unsigned long long curd[kQUnroll];
+                        long long curs[kQUnroll];
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            curd[j] = kInfBits;
+                            curs[j] = -1;
+                            if (wv[j] < 0) continue;
+                            if (kSSSD) {
+                                curd[j] = S.dist[wv[j]];
+                            } else {
+                                DS z = S.ds[wv[j]];
+                                curd[j] = z.d;
+                                curs[j] = z.s;
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            const int w = wv[j];
+                            if (w < 0 || !(nd[j] < as_d(curd[j]))) continue;
+                            bool improved = false, first = false;
+                            if (kSSSD) {
+                                unsigned long long old = atomicMin(&S.dist[w], as_b(nd[j]));
+                                improved = nd[j] < as_d(old);
                                 first = old == kInfBits;
+                            } else {
+                                DS cur;
+                                cur.d = curd[j];
+                                cur.s = curs[j];
+                                while (nd[j] < as_d(cur.d)) {
+                                    DS nw;
+                                    nw.d = as_b(nd[j]);
+                                    nw.s = su;
+                                    DS prev = atomicCAS(&S.ds[w], cur, nw);
+                                    if (prev.d == cur.d && prev.s == cur.s) { improved = true; break; }
+                                    cur = prev;
+                                }
                             }
-                        } else {
-                            DS cur = S.ds[w];
-                            while (nd < as_d(cur.d)) {
-                                DS nw;
-                                nw.d = as_b(nd);
-                                nw.s = su;
-                                DS prev = atomicCAS(&S.ds[w], cur, nw);
-                                if (prev.d == cur.d && prev.s == cur.s) { improved = true; break; }
-                                cur = prev;
+                            if (!improved) continue;
+                            if (kSSSD && first) {
+                                int k = atomicAdd(&s_touchN, 1);
+                                S.touched[k] = w;
                             }
-                        }
-                        if (!improved) continue;
-                        if (kSSSD && first) {
-                            int k = atomicAdd(&s_touchN, 1);
-                            S.touched[k] = w;
-                        }
-                        double f = kSSSD ? nd + hdist(P.pos, w, tgt) : nd;
-                        if (f < thr) {
-                            if (atomicExch(&S.nflag[w], xst) != xst) S.next[atomicAdd(&s_nextN, 1)] = w;
-                        } else if (atomicExch(&S.fflag[w], fst2) != fst2) {
-                            int k = atomicAdd(&s_farN, 1);
-                            if (k < P.list_cap) S.far[k] = w;
-                            else s_overflow = 1;
+                            double f = kSSSD ? nd[j] + hdist(P.pos, w, tgt) : nd[j];
+                            if (f < thr) {
+                                if (atomicExch(&S.nflag[w], xst) != xst) S.next[atomicAdd(&s_nextN, 1)] = w;
+                            } else if (atomicExch(&S.fflag[w], fst2) != fst2) {
+                                int k = atomicAdd(&s_farN, 1);
+                                if (k < P.list_cap) S.far[k] = w;
+                                else s_overflow = 1;
+                            }
                         }
                     }
                 }
@@ -298,6 +335,336 @@ __global__ void __launch_bounds__(kQThreads) k_query(QParams P) {
         }
         if (tid == 0) *stamp_ctr = s_stamp;
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster form: one query per thread-block cluster (8 or 16 SMs).  A batch runs
+// only as many queries at once as there are clusters, so each query's
+// distance and flag arrays stay in L2 while many SMs expand its frontier;
+// per-block query concurrency (the single-block form above) thrashes L2 on
+// large graphs.  The search is the same near-far label-correcting one, with:
+//   * cluster barriers (hardware, no spinning) in place of __syncthreads;
+//   * the phase counters in the first block's shared memory, reached by the
+//     others through distributed shared memory, appended to with one atomic
+//     per warp; each counter is triple-buffered by phase number, so that the
+//     first block resets the copy nobody reads or writes in this phase;
+//   * every decision (leave a loop, move the threshold) taken from values
+//     read after a barrier and not written again before the next one, so all
+//     blocks of a cluster take the same branches and meet at every barrier;
+//   * mutable per-query arrays read through L2 (ld.global.cg): other SMs
+//     write them, and L1 is not coherent across SMs.
+
+#ifndef SVG_QC_THREADS
+#define SVG_QC_THREADS 512
+#endif
+#ifndef SVG_QC_MINB
+#define SVG_QC_MINB 2  // two blocks per SM (64 registers): twice the warps to hide load latency
+#endif
+constexpr int kCThreads = SVG_QC_THREADS;
+
+struct QCtl {
+    unsigned long long fmin[3];  // smallest waiting priority, by threshold move
+    int nearA[3];                // near list filled by the far split
+    int farB[3];                 // far list filled by the split and the drain
+    int nextX[3];                // next near list, by drain round
+    int touch;                   // SSSD: vertices whose distance left +inf
+    int q;                       // query being served
+    int init_far;                // far list length after the sources
+    uint32_t stamp;              // slot stamp at the query's start
+};
+
+// Append the lanes with pred set to a list whose length is *counter (which may
+// live in another block's shared memory): one atomic per warp.  Every lane of
+// the warp must call it.  Returns the lane's position, or -1.
+__device__ __forceinline__ int warp_append(bool pred, int* counter, int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (m == 0) return -1;
+    const int first = __ffs(m) - 1;
+    int base = 0;
+    if (lane == first) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, first);
+    return pred ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+        x = y < x ? y : x;
+    }
+    return x;
+}
+
+__device__ __forceinline__ DS ld_ds(const DS* p) {
+    const longlong2 z = __ldcg(reinterpret_cast<const longlong2*>(p));
+    DS r;
+    r.d = (unsigned long long)z.x;
+    r.s = z.y;
+    return r;
+}
+
+template <bool kSSSD, bool kSrc>
+__global__ void __launch_bounds__(kCThreads, SVG_QC_MINB) k_query_cluster(QParams P) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ QCtl s_ctl;
+    QCtl* ctl = cl.map_shared_rank(&s_ctl, 0);
+    const int csize = (int)cl.num_blocks();
+    const int crank = (int)cl.block_rank();
+    const int slot = (int)blockIdx.x / csize;
+    Slot S = carve_slot(P, slot);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int nthr = csize * kCThreads, gtid = crank * kCThreads + tid;
+    const int gwarp = gtid >> 5, nwarps = nthr >> 5;
+    const bool leader = crank == 0 && tid == 0;
+    const long long round_cap = 64LL * ((long long)P.nv + 16);
+
+    for (;;) {
+        if (leader) {
+            ctl->q = atomicAdd(P.head, 1);
+            ctl->stamp = P.slot_stamp[slot];
+        }
+        cl.sync();
+        const int q = ctl->q;
+        uint32_t stamp = ctl->stamp;
+        cl.sync();  // q and stamp read everywhere before the leader moves on (or any block leaves)
+        if (q >= P.n) break;
+        const int tgt = kSSSD ? P.t[q] : -1;
+
+        // ---------------- initialise
+        if (leader) {
+            for (int k = 0; k < 3; ++k) {
+                ctl->fmin[k] = kInfBits;
+                ctl->nearA[k] = 0;
+                ctl->farB[k] = 0;
+                ctl->nextX[k] = 0;
+            }
+            ctl->touch = 0;
+        }
+        if (!kSSSD) {
+            for (int v = gtid; v < P.nv; v += nthr) {
+                DS z;
+                z.d = kInfBits;
+                z.s = -1;
+                S.ds[v] = z;
+            }
+        }
+        cl.sync();
+        stamp += 1;
+        const uint32_t fst = stamp;
+        if (leader) {
+            int nf = 0;
+            if (kSSSD) {
+                const int s = P.s[q];
+                S.dist[s] = as_b(0.0);
+                S.touched[0] = s;
+                ctl->touch = 1;
+                S.far[nf++] = s;
+                S.fflag[s] = fst;
+            } else {
+                // SVG.cu:358-364: assignments in listed order, the last weight of a repeated source wins
+                const int64_t b = P.set_off[q], e = P.set_off[q + 1];
+                for (int64_t i = b; i < e; ++i) {
+                    DS z;
+                    z.d = as_b(P.weights[i]);
+                    z.s = P.srcs[i];
+                    S.ds[P.srcs[i]] = z;
+                }
+                for (int64_t i = b; i < e; ++i) {
+                    const int v = P.srcs[i];
+                    if (S.fflag[v] != fst) {
+                        S.fflag[v] = fst;
+                        S.far[nf++] = v;
+                    }
+                }
+            }
+            ctl->init_far = nf;
+        }
+        cl.sync();
+        int farN = ctl->init_far;
+        int32_t *far = S.far, *far2 = S.far2, *near = S.near, *next = S.next;
+        long long rounds = 0;
+        int o = 0, gr = 0;
+        bool over = false;
+
+        // ---------------- main loop: move the threshold, drain near frontiers
+        for (;;) {
+            // the far counter keeps counting past the list's capacity, so an
+            // overflow shows in the value every block reads after the barrier
+            if (++rounds > round_cap || farN > P.list_cap) {
+                over = true;
+                break;
+            }
+            const int ob = o % 3;
+            unsigned long long m = kInfBits;
+            for (int i = gtid; i < farN; i += nthr) {
+                const int v = __ldcg(&far[i]);
+                const double d = kSSSD ? as_d(__ldcg(&S.dist[v])) : as_d(ld_ds(&S.ds[v]).d);
+                const double f = kSSSD ? d + hdist(P.pos, v, tgt) : d;
+                m = as_b(f) < m ? as_b(f) : m;
+            }
+            m = warp_min_u64(m);
+            if (lane == 0 && m != kInfBits) atomicMin(&ctl->fmin[ob], m);
+            if (leader) {
+                const int nb = (o + 1) % 3;
+                ctl->fmin[nb] = kInfBits;
+                ctl->nearA[nb] = 0;
+                ctl->farB[nb] = 0;
+            }
+            cl.sync();
+            if (farN == 0) break;
+            const double fmin = as_d(ctl->fmin[ob]);
+            if (kSSSD && as_d(__ldcg(&S.dist[tgt])) <= fmin) break;  // no waiting path can beat the target
+            const double thr = fmin + P.delta;
+            stamp += 2;
+            const uint32_t nst = stamp - 1, fst2 = stamp;
+            // split far: below the threshold -> near, the rest -> far2 (deduplicated)
+            for (int base = gwarp * 32; base < farN; base += nthr) {
+                const int i = base + lane;
+                bool to_near = false, to_far = false;
+                int v = -1;
+                if (i < farN) {
+                    v = __ldcg(&far[i]);
+                    const double d = kSSSD ? as_d(__ldcg(&S.dist[v])) : as_d(ld_ds(&S.ds[v]).d);
+                    const double f = kSSSD ? d + hdist(P.pos, v, tgt) : d;
+                    if (f < thr) to_near = atomicExch(&S.nflag[v], nst) != nst;
+                    else to_far = atomicExch(&S.fflag[v], fst2) != fst2;
+                }
+                int p = warp_append(to_near, &ctl->nearA[ob], lane);
+                if (p >= 0) near[p] = v;
+                p = warp_append(to_far, &ctl->farB[ob], lane);
+                if (p >= 0 && p < P.list_cap) far2[p] = v;
+            }
+            cl.sync();
+            {
+                int32_t* t = far; far = far2; far2 = t;
+            }
+            int nearN = ctl->nearA[ob];
+
+            // drain the near frontier: one warp per vertex, lanes over its edges
+            while (nearN > 0) {
+                if (++rounds > round_cap) {
+                    over = true;
+                    break;
+                }
+                const int gb = gr % 3;
+                stamp += 1;
+                const uint32_t xst = stamp;
+                if (leader) ctl->nextX[(gr + 1) % 3] = 0;
+                for (int i = gwarp; i < nearN; i += nwarps) {
+                    const int u = __ldcg(&near[i]);
+                    double du;
+                    long long su = 0;
+                    if (kSSSD) {
+                        du = as_d(__ldcg(&S.dist[u]));
+                    } else {
+                        const DS z = ld_ds(&S.ds[u]);
+                        du = as_d(z.d);
+                        su = z.s;
+                    }
+                    const int64_t e0 = __ldg(&P.off[u]), e1 = __ldg(&P.off[u + 1]);
+                    for (int64_t eb = e0; eb < e1; eb += 32 * kQUnroll) {
+                        int wv[kQUnroll];
+                        double nd[kQUnroll];
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            const int64_t e = eb + 32 * j + lane;
+                            wv[j] = e < e1 ? __ldg(&P.adj[e]) : -1;
+                            nd[j] = e < e1 ? du + __ldg(&P.w[e]) : 0.0;
+                        }
+                        unsigned long long curd[kQUnroll];
+                        long long curs[kQUnroll];
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            curd[j] = kInfBits;
+                            curs[j] = -1;
+                            if (wv[j] < 0) continue;
+                            if (kSSSD) {
+                                curd[j] = __ldcg(&S.dist[wv[j]]);
+                            } else {
+                                const DS z = ld_ds(&S.ds[wv[j]]);
+                                curd[j] = z.d;
+                                curs[j] = z.s;
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < kQUnroll; ++j) {
+                            const int w = wv[j];
+                            bool to_next = false, to_far = false, to_touch = false;
+                            if (w >= 0 && nd[j] < as_d(curd[j])) {
+                                bool improved = false;
+                                if (kSSSD) {
+                                    const unsigned long long old = atomicMin(&S.dist[w], as_b(nd[j]));
+                                    improved = nd[j] < as_d(old);
+                                    to_touch = old == kInfBits;
+                                } else {
+                                    DS cur;
+                                    cur.d = curd[j];
+                                    cur.s = curs[j];
+                                    while (nd[j] < as_d(cur.d)) {
+                                        DS nw;
+                                        nw.d = as_b(nd[j]);
+                                        nw.s = su;
+                                        const DS prev = atomicCAS(&S.ds[w], cur, nw);
+                                        if (prev.d == cur.d && prev.s == cur.s) {
+                                            improved = true;
+                                            break;
+                                        }
+                                        cur = prev;
+                                    }
+                                }
+                                if (improved) {
+                                    const double f = kSSSD ? nd[j] + hdist(P.pos, w, tgt) : nd[j];
+                                    if (f < thr) to_next = atomicExch(&S.nflag[w], xst) != xst;
+                                    else to_far = atomicExch(&S.fflag[w], fst2) != fst2;
+                                }
+                            }
+                            int p;
+                            if (kSSSD) {
+                                p = warp_append(to_touch, &ctl->touch, lane);
+                                if (p >= 0) S.touched[p] = w;
+                            }
+                            p = warp_append(to_next, &ctl->nextX[gb], lane);
+                            if (p >= 0) next[p] = w;
+                            p = warp_append(to_far, &ctl->farB[ob], lane);
+                            if (p >= 0 && p < P.list_cap) far[p] = w;
+                        }
+                    }
+                }
+                cl.sync();
+                nearN = ctl->nextX[gb];
+                {
+                    int32_t* t = near; near = next; next = t;
+                }
+                ++gr;
+            }
+            if (over) break;
+            farN = ctl->farB[ob];
+            ++o;
+        }
+
+        // ---------------- results (every block got here after the same barriers)
+        const bool ovf = over;
+        if (kSSSD) {
+            if (leader) {
+                const unsigned long long dt = __ldcg(&S.dist[tgt]);
+                P.out[q] = ovf ? -1.0 : (dt == kInfBits ? DBL_MAX : as_d(dt));
+            }
+            cl.sync();  // the target's distance is read before the reset below
+            const int tn = ctl->touch;
+            for (int i = gtid; i < tn; i += nthr) S.dist[__ldcg(&S.touched[i])] = kInfBits;
+        } else {
+            double* od = P.out_dist + (size_t)q * P.nv;
+            int32_t* os = kSrc ? P.out_src + (size_t)q * P.nv : nullptr;
+            for (int v = gtid; v < P.nv; v += nthr) {
+                const DS z = ld_ds(&S.ds[v]);
+                od[v] = z.d == kInfBits ? DBL_MAX : (ovf ? -1.0 : as_d(z.d));
+                if (kSrc) os[v] = (int32_t)z.s;
+            }
+        }
+        if (leader) P.slot_stamp[slot] = stamp;
+        cl.sync();
     }
 }
 
@@ -339,14 +706,88 @@ double graph_delta(svg_graph* g, cudaStream_t st) {
     return g->delta;
 }
 
+namespace {
+#ifndef SVG_QC_CLUSTER
+#define SVG_QC_CLUSTER 16
+#endif
+
+template <bool A, bool B>
+cudaLaunchConfig_t cluster_config(cudaLaunchAttribute* at, int nclusters, int csize, cudaStream_t st) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(nclusters * csize), 1, 1);
+    cfg.blockDim = dim3(kCThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    at->id = cudaLaunchAttributeClusterDimension;
+    at->val.clusterDim.x = (unsigned)csize;
+    at->val.clusterDim.y = 1;
+    at->val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+void allow_large_clusters() {
+    static bool done = false;
+    if (done) return;
+    SVG_CUDA(cudaFuncSetAttribute(k_query_cluster<true, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    SVG_CUDA(cudaFuncSetAttribute(k_query_cluster<false, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    SVG_CUDA(cudaFuncSetAttribute(k_query_cluster<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    done = true;
+}
+
+template <bool A, bool B>
+void launch_cluster(const QParams& P, int nclusters, int csize, cudaStream_t st) {
+    allow_large_clusters();
+    cudaLaunchAttribute at;
+    cudaLaunchConfig_t cfg = cluster_config<A, B>(&at, nclusters, csize, st);
+    SVG_CUDA(cudaLaunchKernelEx(&cfg, k_query_cluster<A, B>, P));
+}
+
+int max_active_clusters(int csize) {
+    allow_large_clusters();
+    cudaLaunchAttribute at;
+    cudaLaunchConfig_t cfg = cluster_config<false, true>(&at, 1, csize, nullptr);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_query_cluster<false, true>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+}  // namespace
+
+// Blocks per query of the cluster form: 16 where such clusters can be
+// scheduled, else 8 (portable).
+int query_cluster_size() {
+    static int cs = 0;
+    if (cs == 0) cs = max_active_clusters(SVG_QC_CLUSTER) >= 1 ? SVG_QC_CLUSTER : 8;
+    return cs;
+}
+
+// Clusters of `csize` blocks that the GPU runs at once.
+int query_cluster_slots(int csize) { return std::max(1, max_active_clusters(csize)); }
+
+// Query blocks one SM holds at once (occupancy of the MSAD kernel, the larger one).
+int query_slots_per_sm() {
+    static int per_sm = 0;
+    if (per_sm <= 0) {
+        int b = 0;
+        SVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_query<false, true>, kQThreads, 0));
+        per_sm = std::max(1, b);
+    }
+    return per_sm;
+}
+
 // Query scratch for `slots` concurrent queries of one graph: per slot the SSSD
 // distances (kept at +inf between queries), the MSAD {dist, src} pairs, the
 // stamp arrays and the frontier lists; one launch at a time may use it.
-svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st) {
+svg_qctx* qctx_create(svg_graph* g, int slots, cudaStream_t st, int cluster) {
     graph_delta(g, st);
     svg_qctx* c = new svg_qctx();
     c->g = g;
     c->slots = std::max(1, slots);
+    c->cluster = std::max(0, cluster);
     const size_t V = (size_t)g->nv;
     c->list_cap = 2 * (int64_t)V + 64;
     c->slot_bytes = al256(8 * V) + al256(16 * V) + 4 * al256(4 * V) + 2 * al256(4 * (size_t)c->list_cap) + al256(4 * V);
@@ -398,7 +839,10 @@ void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, d
     P.t = d_t;
     P.out = d_dist;
     SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
-    k_query<true, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
+    if (c->cluster > 0)
+        launch_cluster<true, false>(P, std::min(n, c->slots), c->cluster, st);
+    else
+        k_query<true, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
     SVG_CUDA(cudaGetLastError());
 }
 
@@ -414,22 +858,32 @@ void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_sr
     P.out_dist = d_dist;
     P.out_src = d_src_id;
     SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
-    if (d_src_id)
-        k_query<false, true><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
-    else
-        k_query<false, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
+    const int nb = std::min(n, c->slots);
+    if (c->cluster > 0) {
+        if (d_src_id) launch_cluster<false, true>(P, nb, c->cluster, st);
+        else launch_cluster<false, false>(P, nb, c->cluster, st);
+    } else if (d_src_id) {
+        k_query<false, true><<<nb, kQThreads, 0, st>>>(P);
+    } else {
+        k_query<false, false><<<nb, kQThreads, 0, st>>>(P);
+    }
     SVG_CUDA(cudaGetLastError());
 }
 
 namespace {
-// The graph's own context for the synchronous batch entry points: two query
-// blocks per SM.
+// The graph's own context for the synchronous batch entry points: as many
+// clusters as run at once (cluster form), or every resident block (plain form).
 svg_qctx* default_ctx(svg_graph* g) {
     if (!g->qdefault) {
-        int dev = 0, sms = 0;
-        SVG_CUDA(cudaGetDevice(&dev));
-        SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        g->qdefault = qctx_create(g, 2 * sms, lib_stream());
+        if (g->qform == SVG_QUERY_PLAIN) {
+            int dev = 0, sms = 0;
+            SVG_CUDA(cudaGetDevice(&dev));
+            SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            g->qdefault = qctx_create(g, query_slots_per_sm() * sms, lib_stream(), 0);
+        } else {
+            const int cs = query_cluster_size();
+            g->qdefault = qctx_create(g, query_cluster_slots(cs), lib_stream(), cs);
+        }
     }
     return g->qdefault;
 }

@@ -37,6 +37,9 @@ double now_s() {
 
 enum ReqKind { kSSSD = 0, kMSAD = 1, kBuild = 2 };
 
+constexpr double kMsadAgeLimit = 0.5;  // s an MSAD may wait while SSSD requests go first
+constexpr int kCopiers = 4;
+
 struct Request {
     int64_t ticket = 0;
     int kind = kSSSD;
@@ -48,8 +51,12 @@ struct Request {
     int status = SVG_OK;
     std::string error;
     double dist = 0.0;
-    std::vector<double> dists;
+    int32_t nres = 0;                 // MSAD: vertices in the result
+    std::vector<double> dists;        // MSAD result, unless the caller gave buffers
     std::vector<int32_t> src_ids;
+    bool into = false;                // MSAD result goes to the caller's buffers (either may be null)
+    double* out_d = nullptr;
+    int32_t* out_s = nullptr;
 };
 
 struct GraphEntry {
@@ -69,7 +76,8 @@ struct Lane {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
     bool busy = false;
-    int kind = 0, graph = -1;
+    bool draining = false;            // results being copied out (worker, unlocked)
+    int kind = 0, graph = -1, nv = 0;
     std::vector<Request*> batch;
     // staging: host pinned and device, fixed at creation
     char* h_in = nullptr;
@@ -96,12 +104,17 @@ struct svg_server {
     std::deque<GraphEntry> graphs;                // deque: entries stay put while the builder runs unlocked
     std::vector<Lane> lanes;
     std::thread worker, builder;
+    std::vector<std::thread> copiers;             // copy finished batches out of pinned staging
+    std::deque<Lane*> copy_q;
+    std::condition_variable cv_copy;
     bool stop = false;
     int64_t next_ticket = 1;
     int64_t resident_bytes = 0;
     // counters
     int64_t batches = 0, batched_requests = 0, evictions = 0, rebuilds = 0;
     int dev = 0;
+    int cluster = 0;  // blocks per query (0: one block)
+    int slots = 1;    // queries a lane serves at once
 };
 
 namespace {
@@ -127,14 +140,23 @@ void finish_request(svg_server* S, Request* r, int status, const std::string& er
 // Launch a batch on a free lane.  Called with S->mu held.
 void launch_batch(svg_server* S, Lane& L) {
     if (S->pending.empty()) return;
+    // short requests first: the oldest SSSD, unless the oldest request is an
+    // MSAD that has waited past the age limit (MSAD cannot starve)
     Request* first = S->pending.front();
+    if (first->kind != kSSSD && now_s() - first->t_submit < kMsadAgeLimit) {
+        for (Request* r : S->pending)
+            if (r->kind == kSSSD) {
+                first = r;
+                break;
+            }
+    }
     const int kind = first->kind, gi = first->graph;
     GraphEntry& G = S->graphs[(size_t)gi];
     const int V = G.g->nv;
     // gather the batch: oldest first, same kind and graph, within staging capacity
     std::vector<Request*> batch;
     size_t in_used = 0, out_used = 0, nsrc = 0;
-    const size_t max_n = (size_t)S->o.max_batch;
+    const size_t max_n = (size_t)(kind == kSSSD ? S->o.max_batch : S->o.max_batch_msad);
     for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < max_n;) {
         Request* r = *it;
         if (r->kind != kind || r->graph != gi) {
@@ -167,7 +189,7 @@ void launch_batch(svg_server* S, Lane& L) {
     L.batch = batch;  // owned by the lane from here on (reported failed if a launch step throws)
     // per-lane context for this graph
     svg_qctx*& ctx = L.ctx[gi];
-    if (!ctx) ctx = qctx_create(G.g, S->o.slots_per_lane, L.st);
+    if (!ctx) ctx = qctx_create(G.g, S->slots, L.st, S->cluster);
     const int n = (int)batch.size();
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     if (kind == kSSSD) {
@@ -209,6 +231,7 @@ void launch_batch(svg_server* S, Lane& L) {
     L.busy = true;
     L.kind = kind;
     L.graph = gi;
+    L.nv = V;
     L.t_launch = now_s();
     G.inflight += 1;
     G.last_used = L.t_launch;
@@ -216,37 +239,69 @@ void launch_batch(svg_server* S, Lane& L) {
     S->batched_requests += n;
 }
 
-// Collect a finished batch.  Called with S->mu held.
-void complete_batch(svg_server* S, Lane& L) {
+// Copy a finished batch's results out of the lane's pinned staging into the
+// requests.  Runs without the lock: the lane is busy and its requests are in
+// neither `pending` nor `done`, so no other thread touches them.
+void copy_results(Lane& L) {
     const int n = (int)L.batch.size();
-    GraphEntry& G = S->graphs[(size_t)L.graph];
-    const double t = now_s();
     if (L.kind == kSSSD) {
         const double* ho = reinterpret_cast<const double*>(L.h_out);
         for (int i = 0; i < n; ++i) {
             Request* r = L.batch[(size_t)i];
             r->dist = ho[i];
             r->status = ho[i] < 0.0 ? SVG_ERR_STATE : SVG_OK;
-            r->t_done = t;
-            S->done[r->ticket] = r;
         }
-    } else {
-        const int V = G.g->nv;
-        const size_t ob = (8 * (size_t)n * V + 255) / 256 * 256;
-        const double* hd = reinterpret_cast<const double*>(L.h_out);
-        const int32_t* hi = reinterpret_cast<const int32_t*>(L.h_out + ob);
-        for (int i = 0; i < n; ++i) {
-            Request* r = L.batch[(size_t)i];
-            r->dists.assign(hd + (size_t)i * V, hd + (size_t)(i + 1) * V);
-            r->src_ids.assign(hi + (size_t)i * V, hi + (size_t)(i + 1) * V);
-            r->status = SVG_OK;
-            r->t_done = t;
-            S->done[r->ticket] = r;
-        }
+        return;
     }
-    G.inflight -= 1;
+    const size_t V = (size_t)L.nv;
+    const size_t ob = (8 * (size_t)n * V + 255) / 256 * 256;
+    const double* hd = reinterpret_cast<const double*>(L.h_out);
+    const int32_t* hi = reinterpret_cast<const int32_t*>(L.h_out + ob);
+    for (int i = 0; i < n; ++i) {
+        Request* r = L.batch[(size_t)i];
+        const double* d = hd + (size_t)i * V;
+        const int32_t* si = hi + (size_t)i * V;
+        if (r->into) {
+            if (r->out_d) std::memcpy(r->out_d, d, 8 * V);
+            if (r->out_s) std::memcpy(r->out_s, si, 4 * V);
+        } else {
+            r->dists.assign(d, d + V);
+            r->src_ids.assign(si, si + V);
+        }
+        r->nres = (int32_t)V;
+        r->status = SVG_OK;
+    }
+}
+
+// Publish a batch whose results were copied.  Called with S->mu held.
+void publish_batch(svg_server* S, Lane& L) {
+    const double t = now_s();
+    for (Request* r : L.batch) {
+        r->t_done = t;
+        S->done[r->ticket] = r;
+    }
+    S->graphs[(size_t)L.graph].inflight -= 1;
     L.batch.clear();
     L.busy = false;
+    L.draining = false;
+}
+
+// launch_batch with its failures reported on the batch's requests.  Called
+// with S->mu held; true if a batch was launched.
+bool launch_guarded(svg_server* S, Lane& L) {
+    try {
+        launch_batch(S, L);
+        return L.busy;
+    } catch (const SvgError& e) {
+        // the batch's requests were taken off `pending`: report them failed
+        for (Request* r : L.batch) finish_request(S, r, e.code, e.msg);
+    } catch (const CudaFail& e) {
+        cudaGetLastError();
+        for (Request* r : L.batch) finish_request(S, r, SVG_ERR_CUDA, e.where);
+    }
+    L.batch.clear();
+    L.busy = false;
+    return false;
 }
 
 void worker_main(svg_server* S) {
@@ -254,29 +309,20 @@ void worker_main(svg_server* S) {
     std::unique_lock<std::mutex> lk(S->mu);
     while (!S->stop) {
         bool progressed = false;
-        for (auto& L : S->lanes) {
-            if (L.busy && cudaEventQuery(L.ev) == cudaSuccess) {
-                complete_batch(S, L);
-                progressed = true;
+        std::vector<Lane*> ready;
+        for (auto& L : S->lanes)
+            if (L.busy && !L.draining && cudaEventQuery(L.ev) == cudaSuccess) {
+                L.draining = true;
+                ready.push_back(&L);
             }
+        if (!ready.empty()) {
+            for (Lane* L : ready) S->copy_q.push_back(L);
+            S->cv_copy.notify_all();
+            progressed = true;
         }
-        if (progressed) S->cv_done.notify_all();
         for (auto& L : S->lanes) {
             if (L.busy || S->pending.empty()) continue;
-            try {
-                launch_batch(S, L);
-                progressed = true;
-            } catch (const SvgError& e) {
-                // the batch's requests were taken off `pending`: report them failed
-                for (Request* r : L.batch) finish_request(S, r, e.code, e.msg);
-                L.batch.clear();
-                L.busy = false;
-            } catch (const CudaFail& e) {
-                cudaGetLastError();
-                for (Request* r : L.batch) finish_request(S, r, SVG_ERR_CUDA, e.where);
-                L.batch.clear();
-                L.busy = false;
-            }
+            progressed |= launch_guarded(S, L);
         }
         bool any_busy = false;
         for (auto& L : S->lanes) any_busy |= L.busy;
@@ -286,6 +332,26 @@ void worker_main(svg_server* S) {
             else
                 S->cv_work.wait_for(lk, std::chrono::milliseconds(5));
         }
+    }
+}
+
+// Copier threads: results of finished batches leave the lane's pinned
+// staging here, off the worker thread, which keeps launching meanwhile.
+void copier_main(svg_server* S) {
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (!S->stop) {
+        if (S->copy_q.empty()) {
+            S->cv_copy.wait_for(lk, std::chrono::milliseconds(5));
+            continue;
+        }
+        Lane* L = S->copy_q.front();
+        S->copy_q.pop_front();
+        lk.unlock();
+        copy_results(*L);
+        lk.lock();
+        publish_batch(S, *L);
+        S->cv_done.notify_all();
+        S->cv_work.notify_all();
     }
 }
 
@@ -319,20 +385,36 @@ bool make_room(svg_server* S, int64_t need, int keep) {
     return true;
 }
 
-// Work a graph needs once before queries (its bucket width), done here on the
-// library stream so that the worker never waits on it while holding the lock.
-svg_status prepare_graph(svg_graph* g, std::string& err) {
+// Work a graph needs once before queries, done unlocked on the library stream
+// so that the worker never waits on it while holding the lock: its bucket
+// width and one query context per lane.
+svg_status prepare_graph(svg_server* S, svg_graph* g, std::string& err, std::vector<svg_qctx*>& ctxs) {
     try {
         graph_delta(g, lib_stream());
+        for (size_t i = 0; i < S->lanes.size(); ++i) ctxs.push_back(qctx_create(g, S->slots, lib_stream(), S->cluster));
     } catch (const SvgError& e) {
         err = e.msg;
+        for (svg_qctx* c : ctxs) qctx_free(c);
+        ctxs.clear();
         return e.code;
     } catch (const CudaFail& e) {
         cudaGetLastError();
         err = std::string("CUDA error ") + cudaGetErrorString(e.err) + " in " + e.where;
+        for (svg_qctx* c : ctxs) qctx_free(c);
+        ctxs.clear();
         return SVG_ERR_CUDA;
     }
     return SVG_OK;
+}
+
+// Hand the prepared contexts to the lanes.  Called with S->mu held.
+void attach_contexts(svg_server* S, int gi, std::vector<svg_qctx*>& ctxs) {
+    for (size_t i = 0; i < ctxs.size() && i < S->lanes.size(); ++i) {
+        svg_qctx*& slot = S->lanes[i].ctx[gi];
+        if (slot) qctx_free(slot);
+        slot = ctxs[i];
+    }
+    ctxs.clear();
 }
 
 void builder_main(svg_server* S) {
@@ -350,7 +432,7 @@ void builder_main(svg_server* S) {
         // admission: the graph's estimated size plus the build's scratch
         svg_build_opts o = G.opts;
         const int64_t est_graph = (int64_t)G.mesh->h.nv * ((int64_t)o.K + 8) * (o.with_paths ? 36 : 12);
-        const int64_t est_ctx = (int64_t)S->lanes.size() * ctx_bytes_nv(G.mesh->h.nv, S->o.slots_per_lane);
+        const int64_t est_ctx = (int64_t)S->lanes.size() * ctx_bytes_nv(G.mesh->h.nv, S->slots);
         const int64_t scratch = std::max<int64_t>(S->o.hbm_budget / 4, (int64_t)64 << 20);
         if (!make_room(S, est_graph + est_ctx + scratch, gi)) {
             // graphs still in use may become evictable: wait for their queries to
@@ -380,12 +462,17 @@ void builder_main(svg_server* S) {
         lk.unlock();
         svg_status st = svg_build(G.mesh, &o, &g);
         std::string err = st == SVG_OK ? "" : svg_last_error();
-        if (st == SVG_OK) st = prepare_graph(g, err);
+        std::vector<svg_qctx*> ctxs;
+        if (st == SVG_OK) {
+            st = prepare_graph(S, g, err, ctxs);
+            if (st != SVG_OK) svg_graph_free(g);
+        }
         lk.lock();
         G.building = false;
         if (st == SVG_OK) {
+            attach_contexts(S, gi, ctxs);
             G.g = g;
-            G.bytes = graph_bytes(g) + (int64_t)S->lanes.size() * ctx_bytes(g, S->o.slots_per_lane);
+            G.bytes = graph_bytes(g) + (int64_t)S->lanes.size() * ctx_bytes(g, S->slots);
             S->resident_bytes += G.bytes;
             G.last_used = now_s();
             for (Request* q : G.waiting) S->pending.push_back(q);
@@ -408,11 +495,13 @@ void svg_server_opts_default(svg_server_opts* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->hbm_budget = (int64_t)40 << 30;
-    o->lanes = 4;
-    o->max_batch = 512;
-    o->slots_per_lane = 74;
+    o->lanes = 0;
+    o->max_batch = 4;
+    o->max_batch_msad = 1;
+    o->slots_per_lane = 0;
+    o->cluster = 0;
     o->staging_in_bytes = (int64_t)16 << 20;
-    o->staging_out_bytes = (int64_t)256 << 20;
+    o->staging_out_bytes = (int64_t)64 << 20;
 }
 
 svg_status svg_server_create(const svg_server_opts* opts, svg_server** out) {
@@ -422,10 +511,27 @@ svg_status svg_server_create(const svg_server_opts* opts, svg_server** out) {
     try {
         if (opts) S->o = *opts;
         else svg_server_opts_default(&S->o);
-        if (S->o.lanes < 1 || S->o.max_batch < 1 || S->o.slots_per_lane < 1 || S->o.staging_in_bytes < 4096 ||
+        if (S->o.lanes < 0 || S->o.max_batch < 1 || S->o.max_batch_msad < 1 || S->o.slots_per_lane < 0 ||
+            S->o.staging_in_bytes < 4096 ||
             S->o.staging_out_bytes < 4096)
             throw SvgError{SVG_ERR_ARG, "bad server options"};
         SVG_CUDA(cudaGetDevice(&S->dev));
+        // kernel form and per-lane concurrency: the lanes share the GPU's resident queries
+        // (blocks in the plain form, clusters otherwise); by default one lane per cluster
+        int resident = 0;
+        if (S->o.cluster < 0) {
+            int sms = 0;
+            SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->dev));
+            S->cluster = 0;
+            resident = query_slots_per_sm() * sms;
+        } else {
+            if (S->o.cluster != 0 && S->o.cluster != 8 && S->o.cluster != 16)
+                throw SvgError{SVG_ERR_ARG, "cluster must be 0, -1, 8 or 16"};
+            S->cluster = S->o.cluster > 0 ? S->o.cluster : query_cluster_size();
+            resident = query_cluster_slots(S->cluster);
+        }
+        if (S->o.lanes == 0) S->o.lanes = std::min(std::max(1, resident), 32);
+        S->slots = S->o.slots_per_lane > 0 ? S->o.slots_per_lane : std::max(1, resident / S->o.lanes);
         S->lanes.resize((size_t)S->o.lanes);
         for (auto& L : S->lanes) {
             SVG_CUDA(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
@@ -439,6 +545,7 @@ svg_status svg_server_create(const svg_server_opts* opts, svg_server** out) {
         }
         S->resident_bytes = (int64_t)S->lanes.size() * (S->o.staging_in_bytes + S->o.staging_out_bytes);
         S->worker = std::thread(worker_main, S);
+        for (int i = 0; i < kCopiers; ++i) S->copiers.emplace_back(copier_main, S);
         S->builder = std::thread(builder_main, S);
     } catch (const SvgError& e) {
         set_error(e.msg);
@@ -462,9 +569,14 @@ void svg_server_free(svg_server* S) {
     }
     S->cv_work.notify_all();
     S->cv_build.notify_all();
+    S->cv_copy.notify_all();
     if (S->worker.joinable()) S->worker.join();
+    for (auto& t : S->copiers)
+        if (t.joinable()) t.join();
     if (S->builder.joinable()) S->builder.join();
     for (auto& L : S->lanes) {
+        for (Request* r : L.batch) delete r;  // batches still on a lane at shutdown
+        L.batch.clear();
         if (L.st) cudaStreamSynchronize(L.st);
         for (auto& kv : L.ctx) qctx_free(kv.second);
         if (L.h_in) cudaFreeHost(L.h_in);
@@ -490,7 +602,8 @@ svg_status svg_server_add_graph(svg_server* S, svg_graph* g, int32_t* graph_id) 
         return SVG_ERR_ARG;
     }
     std::string err;
-    svg_status pst = prepare_graph(g, err);
+    std::vector<svg_qctx*> ctxs;
+    svg_status pst = prepare_graph(S, g, err, ctxs);
     if (pst != SVG_OK) {
         set_error(err);
         return pst;
@@ -502,11 +615,12 @@ svg_status svg_server_add_graph(svg_server* S, svg_graph* g, int32_t* graph_id) 
     G.opts.K = g->K;
     G.g = g;
     G.owned = false;  // the caller's graph: never evicted, never freed by the server
-    G.bytes = graph_bytes(g) + (int64_t)S->lanes.size() * ctx_bytes(g, S->o.slots_per_lane);
+    G.bytes = graph_bytes(g) + (int64_t)S->lanes.size() * ctx_bytes(g, S->slots);
     G.last_used = now_s();
     S->resident_bytes += G.bytes;
     S->graphs.push_back(std::move(G));
     *graph_id = (int32_t)S->graphs.size() - 1;
+    attach_contexts(S, *graph_id, ctxs);
     return SVG_OK;
 }
 
@@ -599,6 +713,23 @@ svg_status svg_server_submit_msad(svg_server* S, int32_t graph_id, int32_t n, co
     return st;
 }
 
+svg_status svg_server_submit_msad_into(svg_server* S, int32_t graph_id, int32_t n, const int32_t* srcs,
+                                       const double* weights, double* dists, int32_t* src_ids, int64_t* ticket) {
+    if (!S || !ticket || n < 0 || (n > 0 && (!srcs || !weights))) return SVG_ERR_ARG;
+    Request* r = new Request();
+    r->kind = kMSAD;
+    r->graph = graph_id;
+    r->srcs.assign(srcs, srcs + n);
+    r->w.assign(weights, weights + n);
+    r->into = true;
+    r->out_d = dists;
+    r->out_s = src_ids;
+    r->t_submit = now_s();
+    svg_status st = submit_query(S, r);
+    if (st == SVG_OK) *ticket = r->ticket;
+    return st;
+}
+
 svg_status svg_server_wait(svg_server* S, int64_t ticket, double timeout_s, svg_server_result* res) {
     if (!S || !res) return SVG_ERR_ARG;
     std::unique_lock<std::mutex> lk(S->mu);
@@ -617,7 +748,7 @@ svg_status svg_server_wait(svg_server* S, int64_t ticket, double timeout_s, svg_
     res->graph_id = r->graph;
     res->latency_ms = (r->t_done - r->t_submit) * 1e3;
     res->dist = r->dist;
-    res->n = (int32_t)r->dists.size();
+    res->n = r->nres;
     return SVG_OK;
 }
 
@@ -651,7 +782,7 @@ svg_status svg_server_poll(svg_server* S, int32_t max, svg_server_result* res, i
         x.graph_id = r->graph;
         x.latency_ms = (r->t_done - r->t_submit) * 1e3;
         x.dist = r->dist;
-        x.n = (int32_t)r->dists.size();
+        x.n = r->nres;
     }
     *n_out = n;
     return SVG_OK;

@@ -93,3 +93,23 @@ def test_unreachable_vertices_report_dbl_max():
     assert np.array_equal(d == DBL_MAX, rd == DBL_MAX)
     fin = rd < DBL_MAX
     assert np.all(np.abs(d[fin] - rd[fin]) <= RTOL * np.maximum(rd[fin], 1e-300))
+
+
+def test_cluster_and_plain_forms_agree(graph):
+    """The cluster form (one query per thread-block cluster) and the plain form
+    (one query per block) give the same distances."""
+    from svg_b200 import QUERY_CLUSTER, QUERY_PLAIN
+    s, m, cm, off, adj, dist = graph
+    rng = np.random.default_rng(5)
+    S = rng.integers(0, m.vertNum, 200).astype(np.int32)
+    T = rng.integers(0, m.vertNum, 200).astype(np.int32)
+    sets = [rng.choice(m.vertNum, k, replace=False).astype(np.int32) for k in (1, 9, 120)]
+    weights = [rng.uniform(0, 0.2, len(x)) for x in sets]
+    out = {}
+    for form in (QUERY_PLAIN, QUERY_CLUSTER):
+        s.set_query_form(form)
+        out[form] = (s.sssd_batch(S, T), s.msad_batch(sets, weights))
+    s.set_query_form(QUERY_CLUSTER)
+    assert np.array_equal(out[QUERY_PLAIN][0], out[QUERY_CLUSTER][0])
+    assert np.array_equal(out[QUERY_PLAIN][1][0], out[QUERY_CLUSTER][1][0])
+    assert (out[QUERY_PLAIN][1][1] == out[QUERY_CLUSTER][1][1]).mean() > 0.999   # equal-distance ties
