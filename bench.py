@@ -406,8 +406,10 @@ def run_serve(args):
     RING = args.ring
     ring_d = [np.zeros(V) for _ in range(RING)]
     ring_s = [np.zeros(V, np.int32) for _ in range(RING)]
-    ring_free = threading.Semaphore(RING)
-    ring_next = [0]
+    import queue
+    ring_free = queue.Queue()
+    for i in range(RING):
+        ring_free.put(i)
     slot_of = {}
     kind_of = {}
     lat = {0: [], 1: []}
@@ -440,7 +442,7 @@ def run_serve(args):
                     samples[i] = r["dist"] if k == 0 else ring_d[slot_of[t]].copy()
                 srv.take(t)
                 if k == 1:
-                    ring_free.release()
+                    ring_free.put(slot_of.pop(t))
                 done_n[0] += 1
             t_done[0] = time.perf_counter()
         finished.set()
@@ -460,9 +462,7 @@ def run_serve(args):
         if kind == 0:
             t = srv.submit_sssd(gid, a, b)
         else:
-            ring_free.acquire()
-            sl = ring_next[0] % RING
-            ring_next[0] += 1
+            sl = ring_free.get()
             t = srv.submit_msad(gid, a, out=(ring_d[sl], ring_s[sl]))
             slot_of[t] = sl
         kind_of[t] = kind
@@ -540,6 +540,166 @@ def run_serve(args):
     return 0
 
 
+def run_mixed(args):
+    """Mixed build + query serving: the pool of 8 meshes (5K..300K vertices,
+    seeds 10-17, tori and height fields), each built once at the start with K
+    drawn from {50, 200}, then further builds of random (mesh, K) pairs
+    arriving as a Poisson stream, interleaved with a Poisson query stream
+    (70 % SSSD, 30 % MSAD with log-uniform set sizes in [1, 1000]) against
+    the graphs already built, all under one device-memory budget with
+    eviction of least-recently-used graphs and rebuild on demand."""
+    import threading
+    _gpu_setup()
+    from svg_b200 import Mesh, Server, meshgen
+    meshes = []
+    for pos, faces in meshgen.pool_meshes(args.scale):
+        m = Mesh.from_arrays(pos, faces)
+        m.copyToGPU()
+        meshes.append(m)
+    Vs = [m.vertNum for m in meshes]
+    rng = np.random.default_rng(4)
+    dur = args.duration
+    ev = []   # (time, kind, payload): kind 0/1 query, 2 build
+    for i in range(len(meshes)):
+        ev.append((0.05 * i, 2, (i, int(rng.choice([50, 200])))))
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / args.build_rate)
+        if t >= dur:
+            break
+        ev.append((t, 2, (int(rng.integers(0, len(meshes))), int(rng.choice([50, 200])))))
+    qa = np.cumsum(rng.exponential(1.0 / args.rate, int(args.rate * dur * 1.3) + 64))
+    qa = qa[(qa < dur) & (qa > 0.5)]   # queries start once the first graphs can be resident
+    kinds = rng.random(len(qa)) < 0.7
+    for ta, k in zip(qa, kinds):
+        ev.append((float(ta), 0 if k else 1, None))
+    ev.sort(key=lambda e: e[0])
+    n_ev = len(ev)
+
+    srv = Server(hbm_budget=int(args.hbm_budget_gb * (1 << 30)), max_batch=args.max_batch,
+                 max_batch_msad=args.max_batch_msad, cluster=args.cluster, staging_in_bytes=16 << 20,
+                 staging_out_bytes=int(args.staging_out_mb) << 20)
+    RING = args.ring
+    vmax = max(Vs)
+    ring_d = [np.zeros(vmax) for _ in range(RING)]
+    ring_s = [np.zeros(vmax, np.int32) for _ in range(RING)]
+    import queue
+    ring_free = queue.Queue()
+    for i in range(RING):
+        ring_free.put(i)
+    slot_of = {}
+    info = {}      # ticket -> (kind, gid)
+    lock = threading.Lock()
+    lat = {0: [], 1: [], 2: []}
+    builds = []
+    failed = [0]
+    gid_mesh = {}
+    done_n = [0]
+    t_done = [0.0]
+    peak_res = [0]
+    finished = threading.Event()
+
+    stop = threading.Event()
+
+    def collector():
+        while done_n[0] < n_ev and not stop.is_set():
+            res = srv.poll(4096)
+            if not res:
+                time.sleep(0.0002)
+                continue
+            for r in res:
+                with lock:
+                    it = info.get(r["ticket"])
+                if it is None:
+                    continue
+                kind, gid = it
+                if r["status"] != 0:
+                    failed[0] += 1
+                else:
+                    lat[kind].append(r["latency_ms"])
+                    if kind == 2:
+                        builds.append((r["edges"], r["build_ms"]))
+                srv.take(r["ticket"])
+                if kind == 1:
+                    with lock:
+                        sl = slot_of.pop(r["ticket"])
+                    ring_free.put(sl)
+                done_n[0] += 1
+            t_done[0] = time.perf_counter()
+        finished.set()
+
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
+    qrng = np.random.default_rng(5)
+    res_ids, res_t = [], [0.0]
+    t0 = time.perf_counter()
+    last_stats = t0
+    for ta, kind, pl in ev:
+        target = t0 + ta
+        now = time.perf_counter()
+        if now < target:
+            time.sleep(max(0.0, target - now - 0.0001))
+            while time.perf_counter() < target:
+                pass
+        if kind == 2:
+            mi, K = pl
+            gid, tk = srv.submit_build(meshes[mi], K)
+            gid_mesh[gid] = mi
+            with lock:
+                info[tk] = (2, gid)
+            continue
+        # the graphs resident now (refreshed every 20 ms)
+        if time.perf_counter() - res_t[0] > 0.02 or not res_ids:
+            res_ids[:] = srv.resident()
+            res_t[0] = time.perf_counter()
+        while not res_ids:   # nothing built yet: the query waits for the first graph
+            time.sleep(0.001)
+            res_ids[:] = srv.resident()
+        gids = res_ids
+        gid = gids[int(qrng.integers(0, len(gids)))]
+        V = Vs[gid_mesh[gid]]
+        if kind == 0:
+            a, b = qrng.integers(0, V, 2)
+            tk = srv.submit_sssd(gid, int(a), int(b))
+        else:
+            k = int(np.clip(np.rint(np.exp(qrng.uniform(0.0, np.log(1000.0)))), 1, 1000))
+            srcs = np.unique(qrng.integers(0, V, k)).astype(np.int32)
+            sl = ring_free.get()
+            tk = srv.submit_msad(gid, srcs, out=(ring_d[sl][:V], ring_s[sl][:V]))
+            with lock:
+                slot_of[tk] = sl
+        with lock:
+            info[tk] = (kind, gid)
+        if time.perf_counter() - last_stats > 0.5:
+            peak_res[0] = max(peak_res[0], srv.stats()["resident_bytes"])
+            last_stats = time.perf_counter()
+    complete = finished.wait(dur * 2 + 120)
+    wall = (t_done[0] if complete else time.perf_counter()) - t0
+    st = srv.stats()
+    stop.set()
+    th.join(5.0)
+    srv.close()
+    nq = len(lat[0]) + len(lat[1])
+    be = sum(e for e, _ in builds)
+    bms = sum(m for _, m in builds)
+    line = {"metric": "mixed_serve_qps", "value": nq / wall, "unit": "req/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "mixed_build_query_pool8", "meshes": Vs, "K_choices": [50, 200],
+                       "hbm_budget_gb": args.hbm_budget_gb, "query_rate_per_s": args.rate,
+                       "build_rate_per_s": args.build_rate, "duration_s": dur, "seed": 4, "scale": args.scale},
+            "wall_s": wall, "queries": nq, "failed": failed[0], "complete": bool(complete),
+            "latency_ms": {"sssd": {"p50": _pct(lat[0], 50), "p99": _pct(lat[0], 99), "n": len(lat[0])},
+                           "msad": {"p50": _pct(lat[1], 50), "p99": _pct(lat[1], 99), "n": len(lat[1])},
+                           "build": {"p50": _pct(lat[2], 50), "p99": _pct(lat[2], 99), "n": len(lat[2])}},
+            "builds": len(builds), "build_edges": be,
+            "build_edges_per_s_device": be / (bms / 1e3) if bms > 0 else None,
+            "builds_per_s": len(builds) / wall,
+            "evictions": st["evictions"], "rebuilds": st["rebuilds"], "resident_graphs_end": st["resident_graphs"],
+            "peak_resident_bytes_sampled": peak_res[0]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,7 +709,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="build", choices=["build", "large", "serve"])
+    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed"])
+    ap.add_argument("--build-rate", type=float, default=2.0, help="mixed: build requests per s")
     ap.add_argument("--scale", type=float, default=1.0, help="large/serve: grid scale of the 750K torus")
     ap.add_argument("--K", default="100,500", help="large: build K values")
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
@@ -572,6 +733,8 @@ def main():
         return run_large(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
 
     ws, rank, local = dist_env()
     import torch

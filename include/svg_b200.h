@@ -236,7 +236,8 @@ typedef struct svg_server_opts {
     int64_t staging_in_bytes;   /* per lane: request inputs (pinned host + device) */
     int64_t staging_out_bytes;  /* per lane: results (an MSAD result is 12 bytes per vertex) */
     int32_t max_batch_msad;     /* MSAD requests per batch (each is a whole-graph search) */
-    int32_t pad_;
+    int32_t build_blocks_per_sm;/* build kernel blocks per SM while serving (the rest of each SM stays free
+                                   for query blocks); 0: as many as fit (fastest build, queries wait) */
 } svg_server_opts;
 
 typedef struct svg_server_result {
@@ -247,6 +248,8 @@ typedef struct svg_server_result {
     int32_t n;                  /* MSAD: number of vertices in the result */
     double latency_ms;          /* submit -> result on the host */
     double dist;                /* SSSD distance (DBL_MAX if unreachable) */
+    int64_t edges;              /* build: SVG edges */
+    double build_ms;            /* build: device time of the build */
 } svg_server_result;
 
 typedef struct svg_server_stats_t {
@@ -282,6 +285,8 @@ svg_status svg_server_poll(svg_server* s, int32_t max, svg_server_result* res, i
 /* Copy an MSAD result (dists[n], src_ids[n], either may be NULL) and release the request. */
 svg_status svg_server_take(svg_server* s, int64_t ticket, double* dists, int32_t* src_ids);
 svg_status svg_server_stats(svg_server* s, svg_server_stats_t* st);
+/* Ids of the graphs resident now (up to max), most recently used first. */
+svg_status svg_server_resident(svg_server* s, int32_t max, int32_t* graph_ids, int32_t* n);
 
 /* Device memory freed by the library (graphs, build scratch, query buffers)
  * is cached for reuse; this returns all cached blocks to CUDA and reports how

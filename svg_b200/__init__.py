@@ -76,12 +76,13 @@ class BuildStats(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget", C.c_int64), ("lanes", C.c_int32), ("max_batch", C.c_int32),
                 ("slots_per_lane", C.c_int32), ("cluster", C.c_int32), ("staging_in_bytes", C.c_int64),
-                ("staging_out_bytes", C.c_int64), ("max_batch_msad", C.c_int32), ("pad", C.c_int32)]
+                ("staging_out_bytes", C.c_int64), ("max_batch_msad", C.c_int32), ("build_blocks_per_sm", C.c_int32)]
 
 
 class ServerResult(C.Structure):
     _fields_ = [("ticket", C.c_int64), ("status", C.c_int32), ("kind", C.c_int32), ("graph_id", C.c_int32),
-                ("n", C.c_int32), ("latency_ms", C.c_double), ("dist", C.c_double)]
+                ("n", C.c_int32), ("latency_ms", C.c_double), ("dist", C.c_double), ("edges", C.c_int64),
+                ("build_ms", C.c_double)]
 
 
 class ServerStats(C.Structure):
@@ -106,7 +107,7 @@ EXPORTS = [
     "svg_server_opts_default", "svg_server_create", "svg_server_free", "svg_server_add_graph",
     "svg_server_submit_build", "svg_server_submit_sssd", "svg_server_submit_msad", "svg_server_wait",
     "svg_server_poll", "svg_server_take", "svg_server_stats", "svg_server_submit_msad_into",
-    "svg_device_memory", "svg_graph_set_query_form",
+    "svg_device_memory", "svg_graph_set_query_form", "svg_server_resident",
 ]
 
 _lib = None
@@ -162,6 +163,7 @@ def lib() -> C.CDLL:
     L.svg_device_memory.argtypes = [C.POINTER(C.c_int64)] * 3 + [C.c_int32]
     L.svg_device_memory.restype = None
     L.svg_graph_set_query_form.argtypes = [_P, C.c_int32]
+    L.svg_server_resident.argtypes = [_P, C.c_int32, _P, C.POINTER(C.c_int32)]
     L.svg_server_wait.argtypes = [_P, C.c_int64, C.c_double, C.POINTER(ServerResult)]
     L.svg_server_poll.argtypes = [_P, C.c_int32, _P, C.POINTER(C.c_int32)]
     L.svg_server_take.argtypes = [_P, C.c_int64, _P, _P]
@@ -444,6 +446,13 @@ class Server:
         n = C.c_int32()
         _check(lib().svg_server_poll(self._h, max_n, C.cast(arr, _P), C.byref(n)))
         return [{k: getattr(arr[i], k) for k, _ in ServerResult._fields_} for i in range(n.value)]
+
+    def resident(self, max_n: int = 4096) -> list:
+        """Graph ids resident now, most recently used first."""
+        ids = np.zeros(max_n, np.int32)
+        n = C.c_int32()
+        _check(lib().svg_server_resident(self._h, max_n, ids.ctypes.data_as(_P), C.byref(n)))
+        return ids[:n.value].tolist()
 
     def stats(self) -> dict:
         st = ServerStats()

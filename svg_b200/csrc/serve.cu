@@ -54,6 +54,8 @@ struct Request {
     int32_t nres = 0;                 // MSAD: vertices in the result
     std::vector<double> dists;        // MSAD result, unless the caller gave buffers
     std::vector<int32_t> src_ids;
+    int64_t edges = 0;                // build: SVG edges
+    double build_ms = 0.0;            // build: device time
     bool into = false;                // MSAD result goes to the caller's buffers (either may be null)
     double* out_d = nullptr;
     int32_t* out_s = nullptr;
@@ -115,6 +117,7 @@ struct svg_server {
     int dev = 0;
     int cluster = 0;  // blocks per query (0: one block)
     int slots = 1;    // queries a lane serves at once
+    int sms = 0;
 };
 
 namespace {
@@ -458,10 +461,18 @@ void builder_main(svg_server* S) {
             continue;
         }
         o.hbm_budget = std::max<int64_t>(S->o.hbm_budget - S->resident_bytes - est_graph - est_ctx, scratch);
+        if (o.blocks <= 0 && S->o.build_blocks_per_sm > 0) o.blocks = S->sms * S->o.build_blocks_per_sm;
         svg_graph* g = nullptr;
         lk.unlock();
         svg_status st = svg_build(G.mesh, &o, &g);
         std::string err = st == SVG_OK ? "" : svg_last_error();
+        if (st == SVG_OK) {
+            svg_build_stats bs{};
+            if (svg_graph_stats(g, &bs) == SVG_OK) {
+                r->edges = bs.edges;
+                r->build_ms = bs.ms_total;
+            }
+        }
         std::vector<svg_qctx*> ctxs;
         if (st == SVG_OK) {
             st = prepare_graph(S, g, err, ctxs);
@@ -498,6 +509,7 @@ void svg_server_opts_default(svg_server_opts* o) {
     o->lanes = 0;
     o->max_batch = 4;
     o->max_batch_msad = 1;
+    o->build_blocks_per_sm = 1;
     o->slots_per_lane = 0;
     o->cluster = 0;
     o->staging_in_bytes = (int64_t)16 << 20;
@@ -516,14 +528,16 @@ svg_status svg_server_create(const svg_server_opts* opts, svg_server** out) {
             S->o.staging_out_bytes < 4096)
             throw SvgError{SVG_ERR_ARG, "bad server options"};
         SVG_CUDA(cudaGetDevice(&S->dev));
+        SVG_CUDA(cudaDeviceGetAttribute(&S->sms, cudaDevAttrMultiProcessorCount, S->dev));
+        if (S->o.build_blocks_per_sm < 0) throw SvgError{SVG_ERR_ARG, "build_blocks_per_sm must be >= 0"};
+        int prio_lo = 0, prio_hi = 0;  // query lanes get the highest stream priority
+        SVG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
         // kernel form and per-lane concurrency: the lanes share the GPU's resident queries
         // (blocks in the plain form, clusters otherwise); by default one lane per cluster
         int resident = 0;
         if (S->o.cluster < 0) {
-            int sms = 0;
-            SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->dev));
             S->cluster = 0;
-            resident = query_slots_per_sm() * sms;
+            resident = query_slots_per_sm() * S->sms;
         } else {
             if (S->o.cluster != 0 && S->o.cluster != 8 && S->o.cluster != 16)
                 throw SvgError{SVG_ERR_ARG, "cluster must be 0, -1, 8 or 16"};
@@ -534,7 +548,7 @@ svg_status svg_server_create(const svg_server_opts* opts, svg_server** out) {
         S->slots = S->o.slots_per_lane > 0 ? S->o.slots_per_lane : std::max(1, resident / S->o.lanes);
         S->lanes.resize((size_t)S->o.lanes);
         for (auto& L : S->lanes) {
-            SVG_CUDA(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
+            SVG_CUDA(cudaStreamCreateWithPriority(&L.st, cudaStreamNonBlocking, prio_hi));
             SVG_CUDA(cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming));
             L.in_bytes = (size_t)S->o.staging_in_bytes;
             L.out_bytes = (size_t)S->o.staging_out_bytes;
@@ -749,6 +763,8 @@ svg_status svg_server_wait(svg_server* S, int64_t ticket, double timeout_s, svg_
     res->latency_ms = (r->t_done - r->t_submit) * 1e3;
     res->dist = r->dist;
     res->n = r->nres;
+    res->edges = r->edges;
+    res->build_ms = r->build_ms;
     return SVG_OK;
 }
 
@@ -783,6 +799,24 @@ svg_status svg_server_poll(svg_server* S, int32_t max, svg_server_result* res, i
         x.latency_ms = (r->t_done - r->t_submit) * 1e3;
         x.dist = r->dist;
         x.n = r->nres;
+        x.edges = r->edges;
+        x.build_ms = r->build_ms;
+    }
+    *n_out = n;
+    return SVG_OK;
+}
+
+svg_status svg_server_resident(svg_server* S, int32_t max, int32_t* ids, int32_t* n_out) {
+    if (!S || !n_out || (max > 0 && !ids)) return SVG_ERR_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    std::vector<std::pair<double, int32_t>> r;
+    for (size_t i = 0; i < S->graphs.size(); ++i)
+        if (S->graphs[i].g) r.emplace_back(-S->graphs[i].last_used, (int32_t)i);
+    std::sort(r.begin(), r.end());
+    int32_t n = 0;
+    for (auto& x : r) {
+        if (n >= max) break;
+        ids[n++] = x.second;
     }
     *n_out = n;
     return SVG_OK;
