@@ -540,6 +540,104 @@ def run_serve(args):
     return 0
 
 
+def run_queries(args):
+    """Batched query kernels on the resident K=100 SVG of the 750K-vertex
+    torus, device buffers only (CUDA events on the library stream): SSSD and
+    MSAD batches in the cluster form and the plain form, and one query per
+    launch in each.  Roofline of the MSAD kernel: per query every edge is
+    relaxed once (4 B adjacency + 8 B length + a 16 B {dist, src} read) and
+    every vertex is initialised, read back and written out (16 + 16 + 12 B)."""
+    torch = _gpu_setup()
+    import svg_b200
+    from svg_b200 import SVG, Mesh, QUERY_CLUSTER, QUERY_PLAIN, meshgen
+    L = svg_b200.lib()
+    P = C.c_void_p
+    pos, faces = meshgen.config_mesh(2, args.scale)
+    mesh = Mesh.from_arrays(pos, faces)
+    mesh.copyToGPU()
+    V = mesh.vertNum
+    svg = SVG()
+    svg.AssignMesh(mesh)
+    svg.SetParameters(100)
+    svg.ConstructSVG(with_paths=False)
+    L.svg_trim_device_cache()
+    _, E, _ = svg.counts()
+    rng = np.random.default_rng(3)
+
+    def mark():
+        x = C.c_double()
+        L.svg_timer_mark(C.byref(x))
+        return x.value
+
+    NS, NM = args.sssd_batch, args.msad_batch
+    S = torch.tensor(rng.integers(0, V, NS), dtype=torch.int32, device="cuda")
+    T = torch.tensor(rng.integers(0, V, NS), dtype=torch.int32, device="cuda")
+    D = torch.empty(NS, dtype=torch.float64, device="cuda")
+    sizes = [int(np.clip(np.rint(np.exp(rng.uniform(0, np.log(1000)))), 1, 1000)) for _ in range(NM)]
+    sets = [np.unique(rng.integers(0, V, k)).astype(np.int32) for k in sizes]
+    off = np.zeros(NM + 1, np.int64)
+    np.cumsum([len(x) for x in sets], out=off[1:])
+    d_off = torch.tensor(off, device="cuda")
+    d_src = torch.tensor(np.concatenate(sets), device="cuda")
+    d_w = torch.zeros(len(d_src), dtype=torch.float64, device="cuda")
+    d_dist = torch.empty(NM * V, dtype=torch.float64, device="cuda")
+    d_sid = torch.empty(NM * V, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def sssd(n, o=0):
+        assert L.svg_sssd_batch_device(svg._g, n, P(S.data_ptr() + 4 * o), P(T.data_ptr() + 4 * o),
+                                       P(D.data_ptr())) == 0
+
+    def msad(n, o=0):
+        assert L.svg_msad_batch_device(svg._g, n, P(d_off.data_ptr() + 8 * o), P(d_src.data_ptr()),
+                                       P(d_w.data_ptr()), P(d_dist.data_ptr()), P(d_sid.data_ptr())) == 0
+
+    def timed(fn, *a):
+        flush.zero_()
+        torch.cuda.synchronize()
+        mark()
+        fn(*a)
+        return mark()
+
+    out = {}
+    for name, form in (("cluster", QUERY_CLUSTER), ("plain", QUERY_PLAIN)):
+        svg.set_query_form(form)
+        sssd(8)
+        msad(2)   # context set-up
+        mark()
+        r = {}
+        r["sssd_single_ms_p50"] = float(np.median([timed(sssd, 1, i) for i in range(args.single)]))
+        r["msad_single_ms_p50"] = float(np.median([timed(msad, 1, i) for i in range(min(args.single, NM))]))
+        ts = [timed(sssd, NS) for _ in range(args.steps)]
+        r["sssd_batch_qps"] = NS / (statistics.mean(ts) / 1e3)
+        tm = [timed(msad, NM) for _ in range(args.steps)]
+        r["msad_batch_ms"] = statistics.mean(tm)
+        r["msad_batch_qps"] = NM / (statistics.mean(tm) / 1e3)
+        out[name] = r
+    svg.set_query_form(QUERY_CLUSTER)
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    peak = peaks.get("hbm_gbs") or 6650.0
+    bytes_q = E * 28.0 + V * 44.0
+    ach = bytes_q * NM / (out["cluster"]["msad_batch_ms"] / 1e3) / 1e9
+    line = {"metric": "msad_batch_qps", "value": out["cluster"]["msad_batch_qps"], "unit": "queries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(LARGE, workload="queries_torus_1000x750_K100", K=100, vertices=V, edges=E,
+                           sssd_batch=NS, msad_batch=NM, msad_set_size="log-uniform [1,1000]", seed=3,
+                           l2="flushed before every timed call (256 MiB write)", scale=args.scale),
+            "forms": out,
+            "msad_batch_speedup_cluster_vs_plain": out["cluster"]["msad_batch_qps"] / out["plain"]["msad_batch_qps"],
+            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach / peak, 4), "traffic": None, "kernel": "k_query_cluster (MSAD)",
+                         "algorithmic_bytes_per_query": bytes_q,
+                         "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_mixed(args):
     """Mixed build + query serving: the pool of 8 meshes (5K..300K vertices,
     seeds 10-17, tori and height fields), each built once at the start with K
@@ -709,7 +807,10 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed"])
+    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed", "queries"])
+    ap.add_argument("--sssd-batch", type=int, default=2048, help="queries: SSSD batch size")
+    ap.add_argument("--msad-batch", type=int, default=96, help="queries: MSAD batch size")
+    ap.add_argument("--single", type=int, default=8, help="queries: one-query launches timed per kind")
     ap.add_argument("--build-rate", type=float, default=2.0, help="mixed: build requests per s")
     ap.add_argument("--scale", type=float, default=1.0, help="large/serve: grid scale of the 750K torus")
     ap.add_argument("--K", default="100,500", help="large: build K values")
@@ -735,6 +836,8 @@ def main():
         return run_serve(args)
     if args.workload == "mixed":
         return run_mixed(args)
+    if args.workload == "queries":
+        return run_queries(args)
 
     ws, rank, local = dist_env()
     import torch

@@ -110,6 +110,7 @@ struct svg_qctx {
     uint32_t* stamps = nullptr;
     int32_t* head = nullptr;
     int cluster = 0;  // blocks per query: a cluster of them, or 0 for one block (the plain form)
+    bool adaptive = false;  // large batches switch to 8-block clusters
 };
 
 namespace svgb {

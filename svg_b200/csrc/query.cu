@@ -766,7 +766,23 @@ int query_cluster_size() {
 }
 
 // Clusters of `csize` blocks that the GPU runs at once.
-int query_cluster_slots(int csize) { return std::max(1, max_active_clusters(csize)); }
+int query_cluster_slots(int csize) {
+    static int cached[17] = {0};
+    if (csize < 1 || csize > 16) return 1;
+    if (cached[csize] <= 0) cached[csize] = std::max(1, max_active_clusters(csize));
+    return cached[csize];
+}
+
+namespace {
+// Cluster size of one call: a context made with `adaptive` serves a batch that
+// fits in the resident clusters of its size at that size (latency), and a
+// larger batch with 8-block clusters, which pack the SMs more fully
+// (throughput); otherwise the context's own size.
+int call_cluster(const svg_qctx* c, int n) {
+    if (!c->adaptive || c->cluster <= 8 || n <= query_cluster_slots(c->cluster)) return c->cluster;
+    return 8;
+}
+}  // namespace
 
 // Query blocks one SM holds at once (occupancy of the MSAD kernel, the larger one).
 int query_slots_per_sm() {
@@ -839,9 +855,10 @@ void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, d
     P.t = d_t;
     P.out = d_dist;
     SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
-    if (c->cluster > 0)
-        launch_cluster<true, false>(P, std::min(n, c->slots), c->cluster, st);
-    else
+    if (c->cluster > 0) {
+        const int cs = call_cluster(c, n);
+        launch_cluster<true, false>(P, std::min(std::min(n, c->slots), query_cluster_slots(cs)), cs, st);
+    } else
         k_query<true, false><<<std::min(n, c->slots), kQThreads, 0, st>>>(P);
     SVG_CUDA(cudaGetLastError());
 }
@@ -860,8 +877,10 @@ void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_sr
     SVG_CUDA(cudaMemsetAsync(P.head, 0, sizeof(int32_t), st));
     const int nb = std::min(n, c->slots);
     if (c->cluster > 0) {
-        if (d_src_id) launch_cluster<false, true>(P, nb, c->cluster, st);
-        else launch_cluster<false, false>(P, nb, c->cluster, st);
+        const int cs = call_cluster(c, n);
+        const int nc = std::min(nb, query_cluster_slots(cs));
+        if (d_src_id) launch_cluster<false, true>(P, nc, cs, st);
+        else launch_cluster<false, false>(P, nc, cs, st);
     } else if (d_src_id) {
         k_query<false, true><<<nb, kQThreads, 0, st>>>(P);
     } else {
@@ -882,7 +901,8 @@ svg_qctx* default_ctx(svg_graph* g) {
             g->qdefault = qctx_create(g, query_slots_per_sm() * sms, lib_stream(), 0);
         } else {
             const int cs = query_cluster_size();
-            g->qdefault = qctx_create(g, query_cluster_slots(cs), lib_stream(), cs);
+            g->qdefault = qctx_create(g, std::max(query_cluster_slots(cs), query_cluster_slots(8)), lib_stream(), cs);
+            g->qdefault->adaptive = true;
         }
     }
     return g->qdefault;
