@@ -294,9 +294,17 @@ class SVG:
         _check(lib().svg_graph_counts(self._g, C.byref(nv), C.byref(nnz), C.byref(K)))
         return nv.value, nnz.value, K.value
 
-    def csr(self):
-        """(offsets[V+1] int64, adj[nnz] int32, dist[nnz] float64) on the host."""
+    def csr(self, out=None):
+        """(offsets[V+1] int64, adj[nnz] int32, dist[nnz] float64) on the host;
+        out=(off, adj, dist) reuses caller arrays (e.g. pinned) of at least that size."""
         nv, nnz, _ = self.counts()
+        if out is not None:
+            off, adj, dist = out
+            assert off.dtype == np.int64 and adj.dtype == np.int32 and dist.dtype == np.float64
+            assert len(off) >= nv + 1 and len(adj) >= nnz and len(dist) >= nnz
+            _check(lib().svg_graph_copy_csr(self._g, off.ctypes.data_as(_P), adj.ctypes.data_as(_P),
+                                            dist.ctypes.data_as(_P)))
+            return off[:nv + 1], adj[:nnz], dist[:nnz]
         off = np.zeros(nv + 1, np.int64)
         adj = np.zeros(max(nnz, 1), np.int32)
         dist = np.zeros(max(nnz, 1))

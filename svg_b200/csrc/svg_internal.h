@@ -3,6 +3,8 @@
 
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "svg_b200.h"
@@ -45,12 +47,34 @@ struct DevMesh {
 };
 
 // Host half-edge construction (Mesh::LoadFromFile semantics).
+// Allocator whose resize() leaves new elements uninitialised: the mesh build
+// writes every element in parallel loops, so the pages are first touched (and
+// faulted in) by many threads instead of by one zero-filling pass.
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <class U>
+    UninitAlloc(const UninitAlloc<U>&) {}
+    template <class U>
+    void construct(U* p) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+
 struct HostMesh {
     int32_t nv = 0, nf = 0, ne = 0;
     std::vector<double> pos;      // 3*nv
     std::vector<int32_t> faces;   // 3*nf
-    std::vector<HeRec> he;
-    std::vector<HeGeo> geo;
+    std::vector<HeRec, UninitAlloc<HeRec>> he;
+    std::vector<HeGeo, UninitAlloc<HeGeo>> geo;
     std::vector<VertRec> vr;
     std::vector<double> angle;
 };
