@@ -540,6 +540,25 @@ def run_serve(args):
     return 0
 
 
+def run_case(args):
+    """One batched build of the 270x270 height field over sources [0, N) with
+    a fixed number of blocks: a small, self-contained launch of the build
+    kernel for profilers (N and the block count bound the device memory)."""
+    _gpu_setup()
+    from svg_b200 import SVG, Mesh, meshgen
+    pos, faces = meshgen.config_mesh(1, args.scale)
+    mesh = Mesh.from_arrays(pos, faces)
+    mesh.copyToGPU()
+    svg = SVG()
+    svg.AssignMesh(mesh)
+    svg.SetParameters(int(args.K.split(",")[0]))
+    n = min(args.sources, mesh.vertNum) if args.sources > 0 else mesh.vertNum
+    st = svg.ConstructSVG(source_begin=0, source_end=n, blocks=args.blocks, heavy_first=0)
+    print(json.dumps({"workload": "case_height_field", "K": svg.K, "sources": n, "blocks": args.blocks,
+                      "stats": st}), flush=True)
+    return 0
+
+
 def run_queries(args):
     """Batched query kernels on the resident K=100 SVG of the 750K-vertex
     torus, device buffers only (CUDA events on the library stream): SSSD and
@@ -807,7 +826,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed", "queries"])
+    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed", "queries", "case"])
+    ap.add_argument("--sources", type=int, default=0, help="case: build sources [0, N)")
+    ap.add_argument("--blocks", type=int, default=0, help="case: build kernel blocks (0 = as many as fit)")
     ap.add_argument("--sssd-batch", type=int, default=2048, help="queries: SSSD batch size")
     ap.add_argument("--msad-batch", type=int, default=96, help="queries: MSAD batch size")
     ap.add_argument("--single", type=int, default=8, help="queries: one-query launches timed per kind")
@@ -838,6 +859,8 @@ def main():
         return run_mixed(args)
     if args.workload == "queries":
         return run_queries(args)
+    if args.workload == "case":
+        return run_case(args)
 
     ws, rank, local = dist_env()
     import torch
