@@ -117,3 +117,22 @@ def test_isolated_vertex_has_no_first_edge():
     faces = np.array([[0, 1, 2]], np.int32)
     ex = Mesh.from_arrays(pos, faces).export()
     assert ex["first_edge"][3] == -1
+
+
+def test_non_manifold_twins_follow_reference_pairing():
+    """Three or more half-edges on one vertex pair (a fin of three triangles, and a
+    face repeated with the same orientation): each later half-edge pairs with the
+    first of its pair and the first keeps the last, as the reference's map does."""
+    from oracle.refbind import RefOracle, ref_available
+    if not ref_available():
+        pytest.skip("reference oracle not built")
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1, 0], [0.5, -1, 0], [0.5, 0, 1], [2, 2, 0]], np.float64)
+    faces = np.array([[0, 1, 2], [1, 0, 3], [0, 1, 4], [1, 2, 5], [1, 2, 5], [2, 0, 4]], np.int32)
+    a = Mesh.from_arrays(pos, faces).export()
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "fin.obj")
+        meshgen.write_obj(p, pos, faces)
+        b = RefOracle().load(p, fix_boundary=True).export()
+    for k in ["he_v0", "he_twin", "he_len", "angle", "first_edge"]:
+        assert np.array_equal(a[k], b[k]), k
+    assert (a["he_twin"] >= 0).sum() >= 8

@@ -173,3 +173,25 @@ def test_builds_evict_and_rebuild_under_budget():
         assert st["resident_graphs"] < 3
     finally:
         srv.close()
+
+
+def test_msad_results_into_caller_buffers(graph):
+    s, m, pos, faces = graph
+    nv = m.vertNum
+    rng = np.random.default_rng(8)
+    sets = [rng.choice(nv, k, replace=False).astype(np.int32) for k in (1, 12, 300)]
+    bufs = [(np.zeros(nv), np.zeros(nv, np.int32)) for _ in sets]
+    srv = Server(hbm_budget=1024 * MB, staging_in_bytes=64 << 10, staging_out_bytes=4 * MB)
+    try:
+        gid = srv.add_graph(s)
+        tk = [srv.submit_msad(gid, x, out=b) for x, b in zip(sets, bufs)]
+        for t in tk:
+            r = srv.wait(t, 300.0)
+            assert r["status"] == 0 and r["n"] == nv
+            srv.take(t)
+    finally:
+        srv.close()
+    d, src = s.msad_batch(sets)
+    for q, (bd, bs) in enumerate(bufs):
+        assert np.array_equal(bd, d[q])
+        assert (bs == src[q]).mean() > 0.999
