@@ -9,8 +9,9 @@
 // batches and launches them; a builder thread runs builds.  Device side: a
 // pool of "lanes", each a CUDA stream with fixed pinned-host and device
 // staging buffers and one query context per resident graph.  A batch is the
-// oldest pending request plus every other pending request of the same kind
-// and graph that fits the lane's staging; requests that arrive while batches
+// oldest queued request (SSSD before MSAD unless an MSAD has waited long)
+// plus the next queued requests of the same kind and graph that fit the lane's
+// staging, taken from that graph's own queue; requests that arrive while batches
 // run are admitted as soon as a lane frees up, and batches on different lanes
 // (and a build on the library stream) overlap on the GPU.
 #include <algorithm>
@@ -72,6 +73,7 @@ struct GraphEntry {
     int64_t bytes = 0;
     int64_t build_ticket = 0;
     std::deque<Request*> waiting;  // queries held while (re)building
+    std::deque<Request*> q[2];     // queued queries of this graph by kind, oldest first
 };
 
 struct Lane {
@@ -100,7 +102,11 @@ struct svg_server {
     svg_server_opts o{};
     std::mutex mu;
     std::condition_variable cv_work, cv_build, cv_done;
-    std::deque<Request*> pending;                 // queries
+    // queued queries: per graph and kind (GraphEntry::q), the oldest-first
+    // order of each kind as tickets (entries no longer in `queued` are skipped),
+    // and the ticket -> request map of everything queued
+    std::deque<int64_t> fifo[2];
+    std::unordered_map<int64_t, Request*> queued;
     std::deque<Request*> builds;                  // build requests (graph index in Request::graph)
     std::unordered_map<int64_t, Request*> done;
     std::deque<GraphEntry> graphs;                // deque: entries stay put while the builder runs unlocked
@@ -140,19 +146,35 @@ void finish_request(svg_server* S, Request* r, int status, const std::string& er
     S->done[r->ticket] = r;
 }
 
+// Queue a query of a resident graph.  Called with S->mu held.
+void enqueue(svg_server* S, Request* r) {
+    S->graphs[(size_t)r->graph].q[r->kind].push_back(r);
+    S->fifo[r->kind].push_back(r->ticket);
+    S->queued[r->ticket] = r;
+}
+
+// Oldest queued request of a kind (nullptr if none).  Called with S->mu held.
+Request* oldest(svg_server* S, int kind) {
+    auto& f = S->fifo[kind];
+    while (!f.empty()) {
+        auto it = S->queued.find(f.front());
+        if (it != S->queued.end()) return it->second;
+        f.pop_front();
+    }
+    return nullptr;
+}
+
+bool graph_has_queued(const GraphEntry& G) { return !G.q[0].empty() || !G.q[1].empty(); }
+
 // Launch a batch on a free lane.  Called with S->mu held.
 void launch_batch(svg_server* S, Lane& L) {
-    if (S->pending.empty()) return;
-    // short requests first: the oldest SSSD, unless the oldest request is an
-    // MSAD that has waited past the age limit (MSAD cannot starve)
-    Request* first = S->pending.front();
-    if (first->kind != kSSSD && now_s() - first->t_submit < kMsadAgeLimit) {
-        for (Request* r : S->pending)
-            if (r->kind == kSSSD) {
-                first = r;
-                break;
-            }
-    }
+    // short requests first: the oldest SSSD, unless the oldest MSAD is older
+    // than it and has waited past the age limit (MSAD cannot starve)
+    Request* so = oldest(S, kSSSD);
+    Request* mo = oldest(S, kMSAD);
+    if (!so && !mo) return;
+    Request* first = so ? so : mo;
+    if (so && mo && mo->t_submit < so->t_submit && now_s() - mo->t_submit >= kMsadAgeLimit) first = mo;
     const int kind = first->kind, gi = first->graph;
     GraphEntry& G = S->graphs[(size_t)gi];
     const int V = G.g->nv;
@@ -160,12 +182,9 @@ void launch_batch(svg_server* S, Lane& L) {
     std::vector<Request*> batch;
     size_t in_used = 0, out_used = 0, nsrc = 0;
     const size_t max_n = (size_t)(kind == kSSSD ? S->o.max_batch : S->o.max_batch_msad);
-    for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < max_n;) {
-        Request* r = *it;
-        if (r->kind != kind || r->graph != gi) {
-            ++it;
-            continue;
-        }
+    auto& gq = G.q[kind];  // this graph's queue of the kind: `first` is at its front
+    while (!gq.empty() && batch.size() < max_n) {
+        Request* r = gq.front();
         size_t in_need, out_need;
         if (kind == kSSSD) {
             in_need = 8;
@@ -177,8 +196,9 @@ void launch_batch(svg_server* S, Lane& L) {
         // 1 KiB slack covers the 256-byte alignment of the packed sections
         if (!batch.empty() && (in_used + in_need + 1024 > L.in_bytes || out_used + out_need + 1024 > L.out_bytes))
             break;
+        gq.pop_front();
+        S->queued.erase(r->ticket);
         if (batch.empty() && (in_need + 1024 > L.in_bytes || out_need + 1024 > L.out_bytes)) {
-            it = S->pending.erase(it);
             finish_request(S, r, SVG_ERR_ARG, "request larger than the serving lane's staging buffers");
             continue;
         }
@@ -186,7 +206,6 @@ void launch_batch(svg_server* S, Lane& L) {
         out_used += out_need;
         nsrc += r->srcs.size();
         batch.push_back(r);
-        it = S->pending.erase(it);
     }
     if (batch.empty()) return;
     L.batch = batch;  // owned by the lane from here on (reported failed if a launch step throws)
@@ -244,7 +263,7 @@ void launch_batch(svg_server* S, Lane& L) {
 
 // Copy a finished batch's results out of the lane's pinned staging into the
 // requests.  Runs without the lock: the lane is busy and its requests are in
-// neither `pending` nor `done`, so no other thread touches them.
+// neither the queues nor `done`, so no other thread touches them.
 void copy_results(Lane& L) {
     const int n = (int)L.batch.size();
     if (L.kind == kSSSD) {
@@ -296,7 +315,7 @@ bool launch_guarded(svg_server* S, Lane& L) {
         launch_batch(S, L);
         return L.busy;
     } catch (const SvgError& e) {
-        // the batch's requests were taken off `pending`: report them failed
+        // the batch's requests were taken off the queues: report them failed
         for (Request* r : L.batch) finish_request(S, r, e.code, e.msg);
     } catch (const CudaFail& e) {
         cudaGetLastError();
@@ -324,7 +343,7 @@ void worker_main(svg_server* S) {
             progressed = true;
         }
         for (auto& L : S->lanes) {
-            if (L.busy || S->pending.empty()) continue;
+            if (L.busy || S->queued.empty()) continue;
             progressed |= launch_guarded(S, L);
         }
         bool any_busy = false;
@@ -365,9 +384,7 @@ bool make_room(svg_server* S, int64_t need, int keep) {
         for (size_t i = 0; i < S->graphs.size(); ++i) {
             GraphEntry& G = S->graphs[i];
             if ((int)i == keep || !G.g || G.inflight > 0 || !G.owned) continue;
-            bool queued = false;
-            for (const Request* q : S->pending) queued |= q->graph == (int)i;
-            if (queued) continue;
+            if (graph_has_queued(G)) continue;
             if (victim < 0 || G.last_used < S->graphs[(size_t)victim].last_used) victim = (int)i;
         }
         if (victim < 0) return false;
@@ -444,8 +461,7 @@ void builder_main(svg_server* S) {
             for (size_t i = 0; i < S->graphs.size(); ++i) {
                 const GraphEntry& H = S->graphs[i];
                 if ((int)i == gi || !H.g || !H.owned) continue;
-                busy |= H.inflight > 0;
-                for (const Request* q : S->pending) busy |= q->graph == (int)i;
+                busy |= H.inflight > 0 || graph_has_queued(H);
             }
             if (busy) {
                 S->builds.push_front(r);
@@ -486,7 +502,7 @@ void builder_main(svg_server* S) {
             G.bytes = graph_bytes(g) + (int64_t)S->lanes.size() * ctx_bytes(g, S->slots);
             S->resident_bytes += G.bytes;
             G.last_used = now_s();
-            for (Request* q : G.waiting) S->pending.push_back(q);
+            for (Request* q : G.waiting) enqueue(S, q);
             G.waiting.clear();
             S->cv_work.notify_all();
         } else {
@@ -602,7 +618,7 @@ void svg_server_free(svg_server* S) {
     }
     for (auto& G : S->graphs)
         if (G.g && G.owned) svg_graph_free(G.g);
-    for (Request* r : S->pending) delete r;
+    for (auto& kv : S->queued) delete kv.second;  // fifo entries are tickets only
     for (Request* r : S->builds) delete r;
     for (auto& kv : S->done) delete kv.second;
     for (auto& G : S->graphs)
@@ -680,7 +696,7 @@ static svg_status submit_query(svg_server* S, Request* r) {
             finish_request(S, r, SVG_ERR_ARG, "vertex out of range");
             return SVG_OK;
         }
-        S->pending.push_back(r);
+        enqueue(S, r);
         S->cv_work.notify_all();
     } else {
         // evicted or still building: hold it, and rebuild if nothing is building it
@@ -825,7 +841,7 @@ svg_status svg_server_resident(svg_server* S, int32_t max, int32_t* ids, int32_t
 svg_status svg_server_stats(svg_server* S, svg_server_stats_t* st) {
     if (!S || !st) return SVG_ERR_ARG;
     std::lock_guard<std::mutex> lk(S->mu);
-    st->pending = (int64_t)S->pending.size();
+    st->pending = (int64_t)S->queued.size();
     st->batches = S->batches;
     st->batched_requests = S->batched_requests;
     st->resident_bytes = S->resident_bytes;
