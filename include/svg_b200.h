@@ -127,7 +127,8 @@ typedef struct svg_build_stats {
 void svg_build_opts_default(svg_build_opts* o);
 
 /* SVG::SetParameters + Allocation + ConstructSVG + Free (SVG.cu:114-182):
- * build the SVG of mesh m on the device.  The graph stays resident. */
+ * build the SVG of mesh m on the device.  The graph stays resident.  Builds
+ * from several threads are safe; they run one at a time. */
 svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out);
 
 svg_status svg_graph_stats(const svg_graph* g, svg_build_stats* st);

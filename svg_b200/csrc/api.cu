@@ -21,7 +21,11 @@ cudaEvent_t g_mark = nullptr;
 void set_error(const std::string& msg) { t_err = msg; }
 
 cudaStream_t lib_stream() {
-    if (!g_stream) SVG_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+    // created once, whichever thread asks first (a serving loop's threads and the caller's)
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] { err = cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking); });
+    if (err != cudaSuccess) throw CudaFail{err, "cudaStreamCreateWithFlags(library stream)"};
     return g_stream;
 }
 
@@ -308,6 +312,10 @@ svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out) {
     return guarded([&]() -> svg_status {
         if (!m || !opts || !out) throw SvgError{SVG_ERR_ARG, "null argument"};
         *out = nullptr;
+        // builds share the lane-scratch arena and run one at a time (a serving
+        // loop's builder thread and a caller's thread may both build)
+        static std::mutex build_mu;
+        std::lock_guard<std::mutex> lock(build_mu);
         svg_graph* g = new svg_graph();
         g->mesh = m;
         try {
