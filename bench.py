@@ -421,9 +421,11 @@ def run_serve(args):
     lag = []
     lock = threading.Lock()
     finished = threading.Event()
+    stop = threading.Event()
+    failed = [0]
 
     def collector():
-        while done_n[0] < n:
+        while done_n[0] < n and not stop.is_set():
             res = srv.poll(4096)
             if not res:
                 time.sleep(0.0002)
@@ -434,11 +436,12 @@ def run_serve(args):
                     i = ticket_req.get(t)
                 if i is None:       # submitted but not yet registered: next poll
                     continue
-                if r["status"] != 0:
-                    raise RuntimeError(f"request {i} failed with status {r['status']}")
                 k = kind_of[t]
-                lat[k].append(r["latency_ms"])
-                if i in want:
+                if r["status"] != 0:
+                    failed[0] += 1
+                else:
+                    lat[k].append(r["latency_ms"])
+                if i in want and r["status"] == 0:
                     samples[i] = r["dist"] if k == 0 else ring_d[slot_of[t]].copy()
                 srv.take(t)
                 if k == 1:
@@ -462,15 +465,17 @@ def run_serve(args):
         if kind == 0:
             t = srv.submit_sssd(gid, a, b)
         else:
-            sl = ring_free.get()
+            sl = ring_free.get(timeout=args.duration * 2 + 120)   # raises instead of waiting for good
             t = srv.submit_msad(gid, a, out=(ring_d[sl], ring_s[sl]))
             slot_of[t] = sl
         kind_of[t] = kind
         with lock:
             ticket_req[t] = i
-    finished.wait(args.duration * 20 + 600)
-    wall = t_done[0] - t0
+    complete = finished.wait(args.duration * 2 + 120)
+    wall = (t_done[0] if complete else time.perf_counter()) - t0
     st1 = srv.stats()
+    stop.set()
+    th.join(5.0)
     srv.close()
 
     # results equal the synchronous batch calls
@@ -510,7 +515,7 @@ def run_serve(args):
     plain_qps = len(allp) / (sum(allp) / 1e3) if allp else None
     alls = single_t[0] + single_t[1]
     alll = lat[0] + lat[1]
-    qps = n / wall
+    qps = (len(lat[0]) + len(lat[1])) / wall
     line = {"metric": "serve_qps", "value": qps, "unit": "req/s", "n_gpus": 1, "steps": 1, "warmup": 1,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(LARGE, workload="serve_torus_1000x750_K100_poisson", K=100, vertices=V,
@@ -518,7 +523,7 @@ def run_serve(args):
                            msad_set_size="log-uniform [1,1000]", seed=3, lanes=args.lanes,
                            max_batch=args.max_batch, max_batch_msad=args.max_batch_msad, slots_per_lane=args.slots,
                            cluster=args.cluster, scale=args.scale),
-            "offered_per_s": n / args.duration, "wall_s": wall,
+            "offered_per_s": n / args.duration, "wall_s": wall, "complete": bool(complete), "failed": failed[0],
             "latency_ms": {"all": {"p50": _pct(alll, 50), "p99": _pct(alll, 99)},
                            "sssd": {"p50": _pct(lat[0], 50), "p99": _pct(lat[0], 99), "n": len(lat[0])},
                            "msad": {"p50": _pct(lat[1], 50), "p99": _pct(lat[1], 99), "n": len(lat[1])}},
@@ -781,7 +786,7 @@ def run_mixed(args):
         else:
             k = int(np.clip(np.rint(np.exp(qrng.uniform(0.0, np.log(1000.0)))), 1, 1000))
             srcs = np.unique(qrng.integers(0, V, k)).astype(np.int32)
-            sl = ring_free.get()
+            sl = ring_free.get(timeout=dur * 2 + 120)   # raises instead of waiting for good
             tk = srv.submit_msad(gid, srcs, out=(ring_d[sl][:V], ring_s[sl][:V]))
             with lock:
                 slot_of[tk] = sl
