@@ -26,6 +26,10 @@
 
 #include "svg_internal.h"
 
+#ifndef SVG_ICH_INLINE_STALE
+#define SVG_ICH_INLINE_STALE 8
+#endif
+
 namespace svgb {
 
 constexpr double kRefPi = 3.141592653589793238;  // Geometry.cuh:18
@@ -818,9 +822,23 @@ struct Lane {
     WinEntry pk_w;
     PsEntry pk_p;
 
+    // Up to this many outdated tops (pseudo-source reborn since the entry was
+    // queued) are popped inside peek() instead of spending a voted step each;
+    // the lane's heap operations happen in the same order either way.
+    static constexpr int kInlineStale = SVG_ICH_INLINE_STALE;
+
     __device__ int peek() {
         if (pk_valid) return pk_act;
         pk_valid = true;
+        for (int inl = 0;; ++inl) {
+            const int a = peek_once();
+            if (a == kActDone || pk_proc || inl >= kInlineStale) return a;
+            if (a == kActWindow) wpop();   // what act_window does with an outdated top
+            else ppop();                   // likewise act_pseudo
+        }
+    }
+
+    __device__ int peek_once() {
         pk_proc = false;
         if (done || (wsize == 0 && psize == 0) || (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined))) {
             done = true;
