@@ -74,74 +74,114 @@ __device__ void record_stats(const Lane& L, const PhaseOut& O, int v) {
     atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[4]), (unsigned long long)L.maxp);
 }
 
-// End of one source in the batched kernel: export the direct candidates.
-// BuildGeodesicPathTo (ICHDevice.cu:336-480) sets pathPassVert on its first
-// hop already: through a vertex that is not the source (enterEdge starts at
-// the vertex, or a window chain whose pseudo-source is another vertex), or
-// through enterEdge -1.  A vertex at distance 0 has no key point at all.
-// The vertex list holds table slots and each vertex slot the split slot of
-// its enter edge, so the walk is direct loads, four entries at a time.
-__device__ void finish_batched(Lane& L, const PhaseOut& O, int v) {
+// End of the sources of the lanes in `amask` (they finished in this step):
+// export each one's direct candidates.  BuildGeodesicPathTo
+// (ICHDevice.cu:336-480) sets pathPassVert on its first hop already: through a
+// vertex that is not the source (enterEdge starts at the vertex, or a window
+// chain whose pseudo-source is another vertex), or through enterEdge -1.  A
+// vertex at distance 0 has no key point at all.  The vertex list holds table
+// slots and each vertex slot the split slot of its enter edge, so the walk is
+// direct loads; the whole warp walks each finished lane's list 32 entries at a
+// time (the other lanes would only wait), and a ballot keeps the candidates
+// in list order.  Every lane of the warp calls it.
+__device__ void finish_warp(Lane& L, const PhaseOut& O, int v, unsigned amask) {
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
     const DevMesh& M = L.C.M;
-    if (L.flags & kFlagCapacity) {
-        int k = atomicAdd(O.retry_n, 1);
-        O.retry[k] = v;
-        return;
-    }
-    unsigned long long base = atomicAdd(O.cand_used, (unsigned long long)L.vcount);
-    record_stats(L, O, v);
-    if (base + (unsigned long long)L.vcount > (unsigned long long)O.cand_cap) {
-        O.cand_n[v] = 0;
-        O.deg[v] = 0;
-        return;  // the host sees cand_used > cand_cap and reruns with a larger pool
-    }
-    int n = 0;
-    for (int i0 = 0; i0 < L.vcount; i0 += 4) {
-        VSlot e[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (i0 + k < L.vcount) e[k] = L.VT[L.VL[i0 + k]];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (i0 + k >= L.vcount) break;
-            const int u = (int)e[k].key;
-            const double d = e[k].dist;
-            if (d == DBL_MAX || u == v) continue;
-            Cand c;
-            c.u = u;
-            c.dist = d;
-            c.ee = -1;
-            c.x = 0.0;
-            bool direct;
-            if (d == 0.0) {
-                direct = true;
-            } else if (e[k].enter == -1) {
-                direct = false;
+    const int warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    unsigned todo = amask;
+    while (todo) {
+        const int o = __ffs(todo) - 1;
+        todo &= todo - 1;
+        // what only the owner knows: retry, pool space, statistics
+        int skip = 0;
+        unsigned long long base = 0;
+        if (lane == o) {
+            if (L.flags & kFlagCapacity) {
+                const int k = atomicAdd(O.retry_n, 1);
+                O.retry[k] = v;
+                skip = 1;
             } else {
-                const int enter = e[k].enter;
-                HeRec h = ld_he(M.he, enter);
-                if (h.v0 == u) {
-                    direct = (h.v1 == v);
-                } else {
-                    const int ss = e[k].sslot >= 0 ? e[k].sslot : L.sfind(enter);
-                    const int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
-                    if ((unsigned)psrc >= (unsigned)M.nv) {
-                        L.flags |= kFlagUndefined;
-                        direct = false;
-                    } else {
-                        direct = (psrc == v);
-                        c.ee = enter;
-                        c.x = L.ST[ss].x;
+                base = atomicAdd(O.cand_used, (unsigned long long)L.vcount);
+                record_stats(L, O, v);
+                if (base + (unsigned long long)L.vcount > (unsigned long long)O.cand_cap) {
+                    O.cand_n[v] = 0;  // the host sees cand_used > cand_cap and reruns with a larger pool
+                    O.deg[v] = 0;
+                    skip = 1;
+                }
+            }
+        }
+        if (__shfl_sync(kFull, skip, o)) continue;
+        base = __shfl_sync(kFull, base, o);
+        const int vo = __shfl_sync(kFull, v, o);
+        const int vcount = __shfl_sync(kFull, L.vcount, o);
+        const uint32_t ep = __shfl_sync(kFull, L.epoch, o);
+        const size_t og = (size_t)(warp_base + o);
+        const int32_t* VL = L.C.vlist + og * (size_t)L.C.vlimit;
+        const VSlot* VT = L.C.vtab + (og << L.C.vcap_log2);
+        const SSlot* ST = L.C.stab + (og << L.C.scap_log2);
+        const uint32_t smask = (1u << L.C.scap_log2) - 1;
+        int n = 0;
+        bool undef = false;
+        for (int i0 = 0; i0 < vcount; i0 += 32) {
+            const int i = i0 + lane;
+            bool direct = false;
+            Cand c;
+            if (i < vcount) {
+                const VSlot e = VT[VL[i]];
+                const int u = (int)e.key;
+                const double d = e.dist;
+                if (d != DBL_MAX && u != vo) {
+                    c.u = u;
+                    c.dist = d;
+                    c.ee = -1;
+                    c.x = 0.0;
+                    if (d == 0.0) {
+                        direct = true;
+                    } else if (e.enter != -1) {
+                        const int enter = e.enter;
+                        const HeRec h = ld_he(M.he, enter);
+                        if (h.v0 == u) {
+                            direct = (h.v1 == vo);
+                        } else {
+                            int ss = e.sslot;
+                            if (ss < 0) {  // the owner's split table, probed as Lane::sfind does
+                                uint32_t hh = (((uint32_t)enter * 0x9E3779B1u) >> (32 - L.C.scap_log2));
+                                for (;;) {
+                                    const uint2 ke = *reinterpret_cast<const uint2*>(&ST[hh]);
+                                    if (ke.y != ep) break;
+                                    if (ke.x == (uint32_t)enter) {
+                                        ss = (int)hh;
+                                        break;
+                                    }
+                                    hh = (hh + 1) & smask;
+                                }
+                            }
+                            const int psrc = ss < 0 ? -1 : ST[ss].psrc;
+                            if ((unsigned)psrc >= (unsigned)M.nv) {
+                                undef = true;
+                            } else {
+                                direct = (psrc == vo);
+                                c.ee = enter;
+                                c.x = ST[ss].x;
+                            }
+                        }
                     }
                 }
             }
-            if (direct) O.cand[base + n++] = c;
+            const unsigned dm = __ballot_sync(kFull, direct);
+            if (direct) O.cand[base + (unsigned long long)(n + __popc(dm & ((1u << lane) - 1u)))] = c;
+            n += __popc(dm);
+        }
+        const bool anyu = __ballot_sync(kFull, undef) != 0;
+        if (lane == o) {
+            if (anyu) L.flags |= kFlagUndefined;
+            O.cand_start[v] = (int64_t)base;
+            O.cand_n[v] = n;
+            O.deg[v] = min(n, L.C.K);
+            if (L.flags & kFlagUndefined) O.st_flags[v] |= 8;
         }
     }
-    O.cand_start[v] = (int64_t)base;
-    O.cand_n[v] = n;
-    O.deg[v] = min(n, L.C.K);
-    if (L.flags & kFlagUndefined) O.st_flags[v] |= 8;
 }
 
 // Longest a lane waits for its action type to be chosen (iterations).
@@ -184,6 +224,7 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
             chosen = (c0 >= c1 && c0 >= c2) ? Lane::kActWindow : (c1 >= c2 ? Lane::kActPseudo : Lane::kActDone);
         }
         const unsigned amask = chosen == Lane::kActWindow ? m0 : (chosen == Lane::kActPseudo ? m1 : m2);
+        if (chosen == Lane::kActDone) finish_warp(L, O, v, amask);  // the whole warp exports
         if (act == chosen) {
             waited = 0;
             if (chosen == Lane::kActWindow) {
@@ -191,7 +232,6 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
             } else if (chosen == Lane::kActPseudo) {
                 L.act_pseudo(amask);
             } else {
-                finish_batched(L, O, v);
                 r = atomicAdd(O.work, 1);
                 v = r < O.nsrc ? O.order[r] : -1;
                 if (v >= 0) L.begin(v, false);
