@@ -210,7 +210,7 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
     if (v >= 0) L.begin(v, false);
     int waited = 0;
     for (;;) {
-        const int act = v >= 0 ? L.peek() : -1;
+        const int act = v >= 0 ? L.template peek<SVG_ICH_INLINE_STALE>() : -1;
         const unsigned m0 = __ballot_sync(kFull, act == Lane::kActWindow);
         const unsigned m1 = __ballot_sync(kFull, act == Lane::kActPseudo);
         const unsigned m2 = __ballot_sync(kFull, act == Lane::kActDone);

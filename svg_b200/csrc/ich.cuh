@@ -326,10 +326,43 @@ struct Lane {
     }
 
     // ----------------------------------------------------------- heaps
-    // Push with the reference's sift-up (PriorityQueue.cuh:48-67): the new
-    // entry moves up while its parent's key is greater.  The first four
-    // ancestors are loaded together and the loop runs over registers, so the
-    // lanes of a warp stay together; deeper climbs continue one level at a time.
+    // The reference's sift-up (PriorityQueue.cuh:57-64): the new entry moves up
+    // while its parent's key is greater.  New windows lie just behind the
+    // propagation front, so their keys are among the smallest in the heap and
+    // they usually climb far.  The first four ancestors are loaded in one
+    // round trip (they are what the level-by-level loop would read: a move
+    // only writes below the next ancestor); the number of moves over them is
+    // counted with the same stop rule and the moves are written predicated, so
+    // no data-dependent branch splits the lanes; a higher climb continues level
+    // by level.
+    template <class T>
+    __device__ __forceinline__ void sift_up(T* H, int cur, const T& x) {
+        T anc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if ((cur >> (j + 1)) > 0) anc[j] = H[cur >> (j + 1)];
+        int m = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (m == j && (cur >> (j + 1)) > 0 && anc[j].key > x.key) m = j + 1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < m) H[cur >> j] = anc[j];
+        int c = cur >> m;
+        if (m == 4) {
+            for (;;) {
+                const int p = c >> 1;
+                if (p == 0) break;
+                const T pe = H[p];
+                if (!(pe.key > x.key)) break;
+                H[c] = pe;
+                c = p;
+            }
+        }
+        H[c] = x;
+    }
+
+    // Push (PriorityQueue.cuh:48-67).
     __device__ void wpush(const NewWin& w, int psrc, int birth) {
         ++generated;  // counts attempts, like numOfWinGen
         if (wsize >= C.wcap) {  // PriorityQueue.cuh:53: dropped when full
@@ -342,33 +375,11 @@ struct Lane {
         }
         const int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
         WP[slot] = w.p;
-        int cur = ++wsize;
-        WinEntry anc[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if ((cur >> (j + 1)) > 0) anc[j] = WH[cur >> (j + 1)];
-        int j = 0;
-        for (; j < 4; ++j) {
-            const int p = cur >> 1;
-            if (p == 0 || !(anc[j].key > w.key)) break;
-            WH[cur] = anc[j];
-            cur = p;
-        }
-        if (j == 4) {
-            for (;;) {
-                const int p = cur >> 1;
-                if (p == 0) break;
-                const WinEntry pe = WH[p];
-                if (!(pe.key > w.key)) break;
-                WH[cur] = pe;
-                cur = p;
-            }
-        }
         WinEntry e;
         e.key = w.key;
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        WH[cur] = e;
+        sift_up(WH, ++wsize, e);
         if (wsize > maxw) maxw = wsize;
     }
     // Pop with the reference's sift-down (PriorityQueue.cuh:76-105): children
@@ -825,8 +836,10 @@ struct Lane {
     // Up to this many outdated tops (pseudo-source reborn since the entry was
     // queued) are popped inside peek() instead of spending a voted step each;
     // the lane's heap operations happen in the same order either way.
-    static constexpr int kInlineStale = SVG_ICH_INLINE_STALE;
-
+    // The batched kernel passes SVG_ICH_INLINE_STALE; a lane stepping on its
+    // own (the plain form) gains nothing from it and passes 0, which compiles
+    // to a single look at the tops.
+    template <int kInlineStale>
     __device__ int peek() {
         if (pk_valid) return pk_act;
         pk_valid = true;
@@ -910,7 +923,7 @@ struct Lane {
     // peek + act for one lane on its own; true when finished.
     __device__ bool step() {
         const unsigned self = 1u << (threadIdx.x & 31);
-        const int a = peek();
+        const int a = peek<0>();
         if (a == kActDone) return true;
         if (a == kActWindow) act_window(self);
         else act_pseudo(self);
