@@ -382,38 +382,44 @@ struct Lane {
         sift_up(WH, ++wsize, e);
         if (wsize > maxw) maxw = wsize;
     }
-    // Pop with the reference's sift-down (PriorityQueue.cuh:76-105): children
-    // of `cur` are compared with each other (ties go right), the smaller moves
+    // The reference's sift-down (PriorityQueue.cuh:76-105): the children of
+    // `cur` are compared with each other (ties go right) and the smaller moves
     // up while it is smaller than the last element.  The children and
     // grandchildren of `cur` are loaded together, so two levels cost one
-    // dependent round trip; reads past the heap's end stay inside the lane's
-    // array (stride >= cap + 4) and are never used.
-    __device__ WinEntry wpop() {
-        WinEntry top = WH[1];
-        WinEntry last = WH[wsize];
-        const int n = --wsize;
+    // dependent round trip (reads past the heap's end stay inside the lane's
+    // array, stride >= cap + 4, and are never used); the two levels are written
+    // with selects and predicated stores, one exit test per two levels.
+    template <class T>
+    __device__ __forceinline__ int sift_down2(T* H, int n, const T& last) {
         int cur = 1;
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
-            const WinEntry a = WH[l], b = WH[l + 1];
+            const T a = H[l], b = H[l + 1];
             const int g = cur << 2;
-            WinEntry q0, q1, q2, q3;
-            if (g <= n) { q0 = WH[g]; q1 = WH[g + 1]; q2 = WH[g + 2]; q3 = WH[g + 3]; }
-            int mc;
-            WinEntry ce;
-            if (l + 1 <= n && !(a.key < b.key)) { mc = l + 1; ce = b; } else { mc = l; ce = a; }
-            if (!(ce.key < last.key)) break;
-            WH[cur] = ce;
-            cur = mc;
-            const int l2 = cur << 1;
-            if (l2 > n) break;
-            const WinEntry c0 = (mc == l) ? q0 : q2, c1 = (mc == l) ? q1 : q3;
-            if (l2 + 1 <= n && !(c0.key < c1.key)) { mc = l2 + 1; ce = c1; } else { mc = l2; ce = c0; }
-            if (!(ce.key < last.key)) break;
-            WH[cur] = ce;
-            cur = mc;
+            T q0, q1, q2, q3;
+            if (g <= n) { q0 = H[g]; q1 = H[g + 1]; q2 = H[g + 2]; q3 = H[g + 3]; }
+            const int k1 = (l + 1 <= n && !(a.key < b.key)) ? 1 : 0;
+            const T e1 = k1 ? b : a;
+            const bool mv1 = e1.key < last.key;
+            const int c1 = l + k1;
+            const int l2 = c1 << 1;
+            const T a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
+            const int k2 = (l2 + 1 <= n && !(a2.key < b2.key)) ? 1 : 0;
+            const T e2 = k2 ? b2 : a2;
+            const bool mv2 = mv1 && l2 <= n && e2.key < last.key;
+            if (mv1) H[cur] = e1;
+            if (mv2) H[c1] = e2;
+            cur = mv2 ? l2 + k2 : (mv1 ? c1 : cur);
+            if (!mv2) break;
         }
+        return cur;
+    }
+    __device__ WinEntry wpop() {
+        WinEntry top = WH[1];
+        WinEntry last = WH[wsize];
+        const int n = --wsize;
+        const int cur = sift_down2(WH, n, last);
         WH[cur] = last;
         WF[nfree++] = (uint16_t)(top.sb & 0xFFFF);
         return top;
@@ -444,28 +450,7 @@ struct Lane {
         PsEntry top = PH[1];
         PsEntry last = PH[psize];
         const int n = --psize;
-        int cur = 1;
-        for (;;) {
-            const int l = cur << 1;
-            if (l > n) break;
-            const PsEntry a = PH[l], b = PH[l + 1];
-            const int g = cur << 2;
-            PsEntry q0, q1, q2, q3;
-            if (g <= n) { q0 = PH[g]; q1 = PH[g + 1]; q2 = PH[g + 2]; q3 = PH[g + 3]; }
-            int mc;
-            PsEntry ce;
-            if (l + 1 <= n && !(a.key < b.key)) { mc = l + 1; ce = b; } else { mc = l; ce = a; }
-            if (!(ce.key < last.key)) break;
-            PH[cur] = ce;
-            cur = mc;
-            const int l2 = cur << 1;
-            if (l2 > n) break;
-            const PsEntry c0 = (mc == l) ? q0 : q2, c1 = (mc == l) ? q1 : q3;
-            if (l2 + 1 <= n && !(c0.key < c1.key)) { mc = l2 + 1; ce = c1; } else { mc = l2; ce = c0; }
-            if (!(ce.key < last.key)) break;
-            PH[cur] = ce;
-            cur = mc;
-        }
+        const int cur = sift_down2(PH, n, last);
         PH[cur] = last;
         return top;
     }
