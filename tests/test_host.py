@@ -136,3 +136,25 @@ def test_non_manifold_twins_follow_reference_pairing():
     for k in ["he_v0", "he_twin", "he_len", "angle", "first_edge"]:
         assert np.array_equal(a[k], b[k]), k
     assert (a["he_twin"] >= 0).sum() >= 8
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_meshes_match_reference_loader(seed):
+    """Random triangles over few vertices (shared, repeated and non-manifold
+    edges, both orientations): half-edge twins, lengths, vertex angles and first
+    edges equal the reference's loader."""
+    from oracle.refbind import RefOracle, ref_available
+    if not ref_available():
+        pytest.skip("reference oracle not built")
+    rng = np.random.default_rng(seed)
+    nv = int(rng.integers(5, 25))
+    nf = int(rng.integers(4, 60))
+    pos = rng.normal(size=(nv, 3))
+    faces = np.array([rng.choice(nv, 3, replace=False) for _ in range(nf)], np.int32)
+    a = Mesh.from_arrays(pos, faces).export()
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "r.obj")
+        meshgen.write_obj(p, pos, faces)
+        b = RefOracle().load(p, fix_boundary=True).export()
+    for k in ["he_v0", "he_twin", "he_len", "angle", "first_edge"]:
+        assert np.array_equal(a[k], b[k]), k
