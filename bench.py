@@ -104,7 +104,7 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = None
@@ -142,6 +142,28 @@ class Clocks:
         busy = [s for s in sm if s > 0.5 * (max(mx) if mx else 0)] or sm
         return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def smi_index(local: int) -> str:
+    """nvidia-smi's name for this process's GPU: the CUDA_VISIBLE_DEVICES entry
+    (an index or a UUID) when that is set, else the local ordinal."""
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local < len(ids):
+            return ids[local]
+    return str(local)
+
+
+def emit(line: dict, args) -> None:
+    """Print the JSON line; with --record also write it to that file."""
+    text = json.dumps(line)
+    print(text, flush=True)
+    if getattr(args, "record", None):
+        d = os.path.dirname(os.path.abspath(args.record))
+        os.makedirs(d, exist_ok=True)
+        with open(args.record, "w") as f:
+            f.write(text + "\n")
 
 
 def workload_mesh():
@@ -298,6 +320,8 @@ def run_large(args):
         return x.value
 
     out = []
+    clocks = Clocks(smi_index(0))
+    clocks.start()
     for K in [int(k) for k in args.K.split(",")]:
         svg = SVG()
         svg.AssignMesh(mesh)
@@ -337,8 +361,10 @@ def run_large(args):
             full = ms / 1e3 * V / n
             row["plain"] = {"sources": n, "build_s": ms / 1e3, "edges": stp["edges"],
                             "est_full_build_s": full, "speedup_batched_vs_plain_est": full / row["build_s"],
-                            "note": f"plain form (64x128 grid, one source per thread) on sources [0,{n}) "
-                                    f"of {V}, time scaled by {V}/{n}"}
+                            "note": (f"plain form (64x128 grid, one source per thread), all {V} sources, measured"
+                                     if n == V else
+                                     f"plain form (64x128 grid, one source per thread) on sources [0,{n}) "
+                                     f"of {V}, time scaled by {V}/{n} (extrapolated)")}
         out.append(row)
         log(json.dumps(row))
     line = {"metric": "svg_build_edges_per_s", "value": out[-1]["edges_per_s"], "unit": "edges/s", "n_gpus": 1,
@@ -346,8 +372,8 @@ def run_large(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(LARGE, workload=f"svg_build_torus_1000x750_value_noise_K{args.K.replace(',', '_')}",
                            vertices=V, scale=args.scale, l2="flushed between steps (256 MiB write)"),
-            "mesh_host_build_and_upload_s": mesh_s, "per_K": out}
-    print(json.dumps(line), flush=True)
+            "mesh_host_build_and_upload_s": mesh_s, "per_K": out, "clocks": clocks.stop()}
+    emit(line, args)
     return 0
 
 
@@ -453,6 +479,8 @@ def run_serve(args):
     th = threading.Thread(target=collector, daemon=True)
     th.start()
     st0 = srv.stats()
+    clocks = Clocks(smi_index(0))
+    clocks.start()
     t0 = time.perf_counter()
     for i, (ta, kind, a, b) in enumerate(reqs):
         target = t0 + ta
@@ -473,6 +501,7 @@ def run_serve(args):
             ticket_req[t] = i
     complete = finished.wait(args.duration * 2 + 120)
     wall = (t_done[0] if complete else time.perf_counter()) - t0
+    ck = clocks.stop()
     st1 = srv.stats()
     stop.set()
     th.join(5.0)
@@ -540,8 +569,131 @@ def run_serve(args):
                                        "latency_ms": {"sssd": {"p50": _pct(single_t[0], 50), "p99": _pct(single_t[0], 99)},
                                                       "msad": {"p50": _pct(single_t[1], 50), "p99": _pct(single_t[1], 99)}}},
             "qps_vs_plain": (qps / plain_qps) if plain_qps else None,
-            "build": {"edges": bst["edges"], "ms": bst["ms_total"]}}
-    print(json.dumps(line), flush=True)
+            "p99_ms_serving_vs_plain": [_pct(alll, 99), _pct(allp, 99)],
+            "build": {"edges": bst["edges"], "ms": bst["ms_total"]},
+            "clocks": ck}
+    emit(line, args)
+    return 0
+
+
+CONFIG0 = dict(workload="svg_build_torus_200x150_K100_sssd100", mesh="torus", R=1.0, r=0.35, grid="200x150",
+               vertices=30000, K=100, seed=0, queries="100 SSSD A*, uniform random pairs (seed 0)")
+
+
+def run_config0(args):
+    """The plain-method configuration: the 30,000-vertex torus (200x150 grid,
+    tube radius jittered by 0.02 r N(0,1), seed 0) built at K=100 by the
+    batched kernel (timed steps), by the plain form (one source per thread,
+    the reference's 64x128 grid and a grid filling every SM) and by the
+    reference's own construction on all host cores (every source); then 100
+    SSSD A* queries on uniform random vertex pairs: one batch through the C
+    ABI (host buffers), one query per launch, and the reference's host A* per
+    query on the graph the reference built (SVG.cu:241-251, 369-413)."""
+    torch = _gpu_setup()
+    import svg_b200
+    from svg_b200 import SVG, Mesh, MODE_PLAIN, meshgen
+    L = svg_b200.lib()
+    K = CONFIG0["K"]
+    pos, faces = meshgen.config_mesh(0)
+    mesh = Mesh.from_arrays(pos, faces)
+    mesh.copyToGPU()
+    V = mesh.vertNum
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def mark():
+        x = C.c_double()
+        L.svg_timer_mark(C.byref(x))
+        return x.value
+
+    def fresh():
+        flush.zero_()
+        torch.cuda.synchronize()
+        mark()
+
+    svg = SVG()
+    svg.AssignMesh(mesh)
+    svg.SetParameters(K)
+    for _ in range(args.warmup):
+        svg.ConstructSVG()
+    clocks = Clocks(smi_index(0))
+    clocks.start()
+    times, st = [], None
+    for _ in range(args.steps):
+        fresh()
+        st = svg.ConstructSVG()
+        times.append(mark())
+    build_ms = statistics.mean(times)
+    plain = {}
+    for name, blocks in (("grid_64x128", 64), ("grid_all_sms", 0)):
+        p = SVG()
+        p.AssignMesh(mesh)
+        p.SetParameters(K)
+        if blocks == 0:
+            per_sm = torch.cuda.get_device_properties(0).multi_processor_count
+            blocks = per_sm * 4
+        fresh()
+        stp = p.ConstructSVG(mode=MODE_PLAIN, blocks=blocks)
+        ms = mark()
+        plain[name] = {"blocks": blocks, "threads_per_block": 128, "build_ms": ms,
+                       "edges_per_s": stp["edges"] / (ms / 1e3), "speedup_batched_vs_plain": ms / build_ms}
+        p.FreeSVGStructure()
+
+    rng = np.random.default_rng(0)
+    s = rng.integers(0, V, 100).astype(np.int32)
+    t = rng.integers(0, V, 100).astype(np.int32)
+    svg.sssd_batch(s[:1], t[:1])   # query context set-up
+    fresh()
+    w0 = time.perf_counter()
+    d_batch = svg.sssd_batch(s, t)
+    batch_wall = (time.perf_counter() - w0) * 1e3
+    batch_dev = mark()
+    per = []
+    for i in range(len(s)):
+        w0 = time.perf_counter()
+        svg.sssd_batch(s[i:i + 1], t[i:i + 1])
+        per.append((time.perf_counter() - w0) * 1e3)
+    ck = clocks.stop()
+    off, nodes = svg.CopySVGToHost()
+
+    cpu = None
+    ref_q = None
+    if not args.no_cpu:
+        # the reference's own construction and A* (test oracle; reported baseline only)
+        from oracle.refbind import RefOracle, ref_available
+        if ref_available():
+            td = tempfile.mkdtemp()
+            obj = os.path.join(td, "m.obj")
+            meshgen.write_obj(obj, pos, faces)
+            rm = RefOracle().load(obj, fix_boundary=True)
+            cores = os.cpu_count() or 1
+            rows = rm.build(K, None, threads=cores)
+            edges = int(rows.tails.sum())
+            cpu = {"value": edges / rows.seconds, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"all {V} sources, the reference's per-source loop incl. its O(V) emission scan",
+                   "seconds": rows.seconds, "edges": edges}
+            dq, secs = rm.sssd(K, rows.tails, rows.nodes, s, t)
+            same_graph = bool(np.array_equal(np.diff(off), rows.tails))
+            rel = np.abs(d_batch - dq) / np.maximum(dq, 1e-300)
+            ref_q = {"host_ms_per_query": secs * 1e3 / len(s), "host_total_ms": secs * 1e3, "cores": 1,
+                     "max_rel_diff_vs_gpu": float(rel.max()), "identical": int((d_batch == dq).sum()),
+                     "graph_degrees_identical": same_graph}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": "oracle/_ref not built"}
+    line = {"metric": METRIC, "value": st["edges"] / (build_ms / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": build_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG0, l2="flushed between steps (256 MiB write)", edges_per_build=st["edges"],
+                           windows_per_build=st["windows"]),
+            "build_ms_all": times, "plain": plain, "cpu_baseline": cpu,
+            "sssd": {"n": len(s), "batch_device_ms": batch_dev, "batch_wall_ms": batch_wall,
+                     "one_per_launch_wall_ms": {"mean": statistics.mean(per), "p50": _pct(per, 50),
+                                                "p99": _pct(per, 99)},
+                     "reference_host": ref_q},
+            "clocks": ck,
+            "flags": {k: st[k] for k in ("queue_drop_sources", "ref_overflow_sources", "watchdog_sources",
+                                         "undefined_sources", "retried_sources")}}
+    emit(line, args)
     return 0
 
 
@@ -624,6 +776,8 @@ def run_queries(args):
         return mark()
 
     out = {}
+    clocks = Clocks(smi_index(0))
+    clocks.start()
     for name, form in (("cluster", QUERY_CLUSTER), ("plain", QUERY_PLAIN)):
         svg.set_query_form(form)
         sssd(8)
@@ -639,6 +793,7 @@ def run_queries(args):
         r["msad_batch_qps"] = NM / (statistics.mean(tm) / 1e3)
         out[name] = r
     svg.set_query_form(QUERY_CLUSTER)
+    ck = clocks.stop()
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
@@ -657,8 +812,9 @@ def run_queries(args):
             "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": None, "kernel": "k_query_cluster (MSAD)",
                          "algorithmic_bytes_per_query": bytes_q,
-                         "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"}}
-    print(json.dumps(line), flush=True)
+                         "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"},
+            "clocks": ck}
+    emit(line, args)
     return 0
 
 
@@ -752,6 +908,8 @@ def run_mixed(args):
 
     th = threading.Thread(target=collector, daemon=True)
     th.start()
+    clocks = Clocks(smi_index(0))
+    clocks.start()
     qrng = np.random.default_rng(5)
     res_ids, res_t = [], [0.0]
     t0 = time.perf_counter()
@@ -797,6 +955,7 @@ def run_mixed(args):
             last_stats = time.perf_counter()
     complete = finished.wait(dur * 2 + 120)
     wall = (t_done[0] if complete else time.perf_counter()) - t0
+    ck = clocks.stop()
     st = srv.stats()
     stop.set()
     th.join(5.0)
@@ -817,8 +976,8 @@ def run_mixed(args):
             "build_edges_per_s_device": be / (bms / 1e3) if bms > 0 else None,
             "builds_per_s": len(builds) / wall,
             "evictions": st["evictions"], "rebuilds": st["rebuilds"], "resident_graphs_end": st["resident_graphs"],
-            "peak_resident_bytes_sampled": peak_res[0]}
-    print(json.dumps(line), flush=True)
+            "peak_resident_bytes_sampled": peak_res[0], "clocks": ck}
+    emit(line, args)
     return 0
 
 
@@ -831,7 +990,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="build", choices=["build", "large", "serve", "mixed", "queries", "case"])
+    ap.add_argument("--workload", default="build", choices=["build", "config0", "large", "serve", "mixed", "queries", "case"])
     ap.add_argument("--sources", type=int, default=0, help="case: build sources [0, N)")
     ap.add_argument("--blocks", type=int, default=0, help="case: build kernel blocks (0 = as many as fit)")
     ap.add_argument("--sssd-batch", type=int, default=2048, help="queries: SSSD batch size")
@@ -853,9 +1012,12 @@ def main():
     ap.add_argument("--ring", type=int, default=256)
     ap.add_argument("--plain-requests", type=int, default=400)
     ap.add_argument("--plain-seconds", type=float, default=30.0)
+    ap.add_argument("--record", default="", help="also write the JSON line to this file")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "config0":
+        return run_config0(args)
     if args.workload == "large":
         return run_large(args)
     if args.workload == "serve":
@@ -904,7 +1066,7 @@ def main():
         timed_build()
     barrier(dist)
     torch.cuda.synchronize()
-    clocks = Clocks(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    clocks = Clocks(smi_index(local))
     clocks.start()
     times, kern, edges, launches = [], [], 0, 0
     st = None

@@ -39,9 +39,11 @@ def build_oracles(ref: bool = True) -> None:
     """Compile the C restatement (always) and the reference oracle (when the
     reference sources are present)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if ref and os.path.isdir(os.environ.get("SVG_REFERENCE_DIR", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref",
-                        "REF=" + os.environ.get("SVG_REFERENCE_DIR", "/root/reference")], check=True)
+    if ref:
+        # the Makefile's REF names where the reference is checked out;
+        # SVG_REFERENCE_DIR overrides it
+        src = os.environ.get("SVG_REFERENCE_DIR")
+        subprocess.run(["make", "-s", "-C", HERE, "ref"] + (["REF=" + src] if src else []), check=True)
 
 
 def ref_available() -> bool:

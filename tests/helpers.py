@@ -60,3 +60,59 @@ def svg_file_bytes(off: np.ndarray, nodes: np.ndarray) -> bytes:
         parts.append(np.int32(off[r + 1] - off[r]).tobytes())
         parts.append(nodes[off[r]:off[r + 1]].tobytes())
     return b"".join(parts)
+
+
+def csr_from_padded(tails: np.ndarray, nodes: np.ndarray):
+    """Padded reference rows -> (offsets, packed nodes), vectorised for full meshes."""
+    tails = np.asarray(tails)
+    off = np.zeros(len(tails) + 1, np.int64)
+    np.cumsum(tails, out=off[1:])
+    mask = np.arange(nodes.shape[1])[None, :] < tails[:, None]
+    return off, nodes[mask]
+
+
+def first_row_mismatches(off_a, nodes_a, off_b, nodes_b,
+                         fields=("adj", "dist", "src_edge", "dst_edge", "src_x", "dst_x"), limit=10):
+    """Bit-exact comparison of two CSR row sets over every row at once.
+    Returns [] when identical, else up to `limit` (row, reason) entries."""
+    if len(off_a) != len(off_b):
+        return [(-1, f"row count {len(off_a) - 1} vs {len(off_b) - 1}")]
+    deg_a, deg_b = np.diff(off_a), np.diff(off_b)
+    bad_deg = np.nonzero(deg_a != deg_b)[0]
+    if len(bad_deg):
+        return [(int(r), f"degree {deg_a[r]} vs {deg_b[r]}") for r in bad_deg[:limit]]
+    out = []
+    row_of = np.repeat(np.arange(len(deg_a)), deg_a)
+    for f in fields:
+        x, y = nodes_a[f], nodes_b[f]
+        eq = x == y
+        if x.dtype.kind == "f":
+            eq |= np.isnan(x) & np.isnan(y)
+        diff = np.nonzero(~eq)[0]
+        if len(diff):
+            rows = np.unique(row_of[diff])[:limit]
+            out += [(int(r), f) for r in rows]
+    return out[:limit]
+
+
+def tree_certified(tails, adj, w, dist, src, sources, weights):
+    """Local certificate of a multi-source shortest-path labelling: every
+    reached vertex v is a source carrying its own id and weight, or has an
+    in-edge (u -> v) with dist[u] + w == dist[v] and src[u] == src[v].  Edge
+    weights are positive, so following such edges back ends at the source
+    src[v]: that source's tree reaches v at exactly dist[v].  Returns the
+    boolean array of certified vertices (unreached vertices count as certified).
+    tails[i] is the row (tail vertex) of CSR edge i."""
+    V = len(dist)
+    u = tails
+    ok_edge = (dist[u] + w == dist[adj]) & (src[u] == src[adj]) & (dist[u] < np.finfo(np.float64).max)
+    cert = np.zeros(V, bool)
+    cert[adj[ok_edge]] = True
+    last_w = {}
+    for s_, w_ in zip(sources, weights):
+        last_w[int(s_)] = float(w_)  # a repeated source keeps its last weight
+    for s_, w_ in last_w.items():
+        if src[s_] == s_ and dist[s_] == w_:
+            cert[s_] = True
+    cert |= dist == np.finfo(np.float64).max
+    return cert

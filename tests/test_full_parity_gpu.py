@@ -1,0 +1,207 @@
+"""Whole-build parity on the benchmark meshes (GPU).
+
+Every row of a full build - neighbour ids, edge lengths and path-end fields -
+must be bit-identical to the reference's own construction (oracle/_ref: the
+reference's ICH compiled as host C++, run on all host cores; the plain-C
+restatement stands in where it is not built):
+  * the 72,900-vertex height field at K=500, the timed benchmark build, where
+    about half the sources fill the reference's 1023-window queue and drop
+    pushes (PriorityQueue.cuh:53), so drop order decides which windows exist;
+  * the 30,000-vertex torus at K=100 (batched and plain forms);
+  * 2,000 seeded sources of the 750,000-vertex torus at K=100 and K=500, built
+    through source ranges.
+Queries on the resident K=100 SVG of the 750K torus: 100 SSSD pairs and 10
+MSAD sets (sizes log-uniform in [1, 1000]) against the oracle's A* and
+Dijkstra (SVG.cu:241-413), distances within 1e-8 relative.  An MSAD vertex may
+name a different source than the oracle only at an exact distance tie; each
+such vertex is logged and certified (both labellings are consistent
+shortest-path forests reaching it at the same distance).
+"""
+import os
+import tempfile
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from oracle.refbind import CpuOracle, RefOracle, ref_available
+from svg_b200 import MODE_BATCHED, MODE_PLAIN, SVG, Mesh, meshgen
+from svg_b200.build_ext import build as build_lib
+from tests.helpers import csr_from_padded, first_row_mismatches, tree_certified
+
+pytestmark = pytest.mark.gpu
+
+CORES = os.cpu_count() or 1
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    build_lib()
+
+
+def _oracle_mesh(pos, faces, td):
+    """The reference's own loader and ICH where built, else the restatement."""
+    if ref_available():
+        obj = os.path.join(td, "m.obj")
+        meshgen.write_obj(obj, pos, faces)
+        return RefOracle().load(obj, fix_boundary=True), "reference"
+    return CpuOracle().mesh(pos, faces), "restatement"
+
+
+def _gpu(pos, faces, K, mode=MODE_BATCHED, **kw):
+    m = Mesh.from_arrays(pos, faces)
+    s = SVG()
+    s.AssignMesh(m)
+    s.SetParameters(K, 10, 2)
+    st = s.ConstructSVG(mode=mode, **kw)
+    off, nodes = s.CopySVGToHost()
+    return off, nodes, st, s, m
+
+
+def _oracle_stats_line(rows):
+    st = rows.stats
+    # ref_driver stats: numOfWinGen, maxWinQSize, maxPseudoQSize, totalCalcVertNum
+    full_q = int((st[:, 1] >= 1023).sum())
+    return f"oracle: {int(st[:, 0].sum())} windows generated, {full_q} sources reached the 1023 queue cap"
+
+
+@pytest.mark.parametrize("cfg,K,modes", [(1, 500, (MODE_BATCHED,)), (0, 100, (MODE_BATCHED, MODE_PLAIN))])
+def test_full_build_identical_to_reference(cfg, K, modes):
+    pos, faces = meshgen.config_mesh(cfg)
+    with tempfile.TemporaryDirectory() as td:
+        om, kind = _oracle_mesh(pos, faces, td)
+        t0 = time.perf_counter()
+        rows = om.build(K, None, threads=CORES)
+        t_or = time.perf_counter() - t0
+    ooff, onodes = csr_from_padded(rows.tails, rows.nodes)
+    del rows.nodes
+    print(f"config {cfg} K={K}: {kind} oracle on {CORES} cores {t_or:.1f} s, {len(ooff) - 1} rows, "
+          f"{ooff[-1]} edges; " + _oracle_stats_line(rows))
+    for mode in modes:
+        off, nodes, st, s, _ = _gpu(pos, faces, K, mode)
+        bad = first_row_mismatches(off, nodes, ooff, onodes)
+        print(f"  {'batched' if mode == MODE_BATCHED else 'plain'}: {st['edges']} edges, "
+              f"{st['queue_drop_sources']} queue-drop sources, {st['retried_sources']} retried, "
+              f"{st['ref_overflow_sources']} ref-overflow, {st['watchdog_sources']} watchdog, "
+              f"{st['undefined_sources']} undefined; mismatching rows: {len(bad)}")
+        assert bad == [], bad
+        assert st["windows_generated"] == int(rows.stats[:, 0].sum())
+        assert st["watchdog_sources"] == 0 and st["undefined_sources"] == 0 and st["ref_overflow_sources"] == 0
+        if cfg == 1:
+            # the cap binds on this mesh: the drop order is exercised
+            assert st["queue_drop_sources"] > 1000
+        s.FreeSVGStructure()
+
+
+@pytest.fixture(scope="module")
+def torus750k():
+    return meshgen.config_mesh(2)
+
+
+@pytest.fixture(scope="module")
+def torus750k_oracle(torus750k):
+    pos, faces = torus750k
+    with tempfile.TemporaryDirectory() as td:
+        yield _oracle_mesh(pos, faces, td)
+
+
+def _sample_ranges(V, n_ranges=4, length=500, seed=20):
+    rng = np.random.default_rng(seed)
+    starts = np.sort(rng.choice(V // length, n_ranges, replace=False)) * length
+    return [(int(a), int(a) + length) for a in starts]
+
+
+@pytest.mark.parametrize("K", [100, 500])
+def test_large_torus_source_sample_identical_to_reference(torus750k, torus750k_oracle, K):
+    pos, faces = torus750k
+    om, kind = torus750k_oracle
+    V = len(pos)
+    ranges = _sample_ranges(V)
+    src = np.concatenate([np.arange(a, b, dtype=np.int32) for a, b in ranges])
+    rows = om.build(K, src, threads=CORES)
+    ooff, onodes = csr_from_padded(rows.tails, rows.nodes)
+    m = Mesh.from_arrays(pos, faces)
+    r0 = 0
+    total_bad = 0
+    drops = 0
+    for a, b in ranges:
+        s = SVG()
+        s.AssignMesh(m)
+        s.SetParameters(K)
+        st = s.ConstructSVG(source_begin=a, source_end=b)
+        drops += st["queue_drop_sources"]
+        off, nodes = s.CopySVGToHost()
+        sub_off = off[a:b + 1] - off[a]
+        got = nodes[off[a]:off[b]]
+        n = b - a
+        want_off = ooff[r0:r0 + n + 1] - ooff[r0]
+        want = onodes[ooff[r0]:ooff[r0 + n]]
+        bad = first_row_mismatches(sub_off, got, want_off, want)
+        total_bad += len(bad)
+        assert bad == [], (a, b, bad)
+        assert off[-1] == off[b] - off[a]
+        r0 += n
+        s.FreeSVGStructure()
+    print(f"750K torus K={K}: {len(src)} sources in ranges {ranges} vs the {kind} oracle; "
+          f"{drops} queue-drop sources; mismatching rows {total_bad}; " + _oracle_stats_line(rows))
+
+
+def _parallel_sssd(cm, off, adj, w, s, t):
+    chunks = np.array_split(np.arange(len(s)), min(CORES, len(s)))
+    out = np.zeros(len(s))
+
+    def run(ix):
+        d, _ = cm.sssd(off, adj, w, s[ix], t[ix])
+        out[ix] = d
+
+    with ThreadPoolExecutor(len(chunks)) as ex:
+        list(ex.map(run, chunks))
+    return out
+
+
+def test_queries_on_large_torus_graph_match_oracle(torus750k):
+    pos, faces = torus750k
+    V = len(pos)
+    m = Mesh.from_arrays(pos, faces)
+    g = SVG()
+    g.AssignMesh(m)
+    g.SetParameters(100)
+    g.ConstructSVG(with_paths=False)
+    off, adj, w = g.csr()
+    cm = CpuOracle().mesh(pos, faces)
+    rng = np.random.default_rng(3)
+
+    s = rng.integers(0, V, 100).astype(np.int32)
+    t = rng.integers(0, V, 100).astype(np.int32)
+    d = g.sssd_batch(s, t)
+    ref = _parallel_sssd(cm, off, adj, w, s, t)
+    rel = np.abs(d - ref) / np.maximum(ref, 1e-300)
+    print(f"SSSD: 100 pairs, max relative difference {rel.max():.3e}, identical {int((d == ref).sum())}")
+    assert np.all(rel <= 1e-8)
+
+    sizes = np.floor(np.exp(rng.uniform(0.0, np.log(1000.0), 10))).astype(int)
+    sets = [rng.choice(V, int(k), replace=False).astype(np.int32) for k in sizes]
+    wts = [rng.uniform(0.0, 0.05, len(x)) for x in sets]
+    dg, sg = g.msad_batch(sets, wts)
+
+    def oracle_msad(q):
+        return cm.msad(off, adj, w, sets[q], wts[q])
+
+    with ThreadPoolExecutor(min(CORES, len(sets))) as ex:
+        outs = list(ex.map(oracle_msad, range(len(sets))))
+    tails = np.repeat(np.arange(V, dtype=np.int32), np.diff(off))  # edge -> its row (tail vertex)
+    for q, (do, so, _) in enumerate(outs):
+        rel = np.abs(dg[q] - do) / np.maximum(do, 1e-300)
+        assert np.all(rel <= 1e-8), (q, rel.max())
+        mism = np.nonzero(sg[q] != so)[0]
+        if len(mism):
+            tie = np.abs(dg[q][mism] - do[mism]) <= 1e-12 * do[mism]
+            cert_g = tree_certified(tails, adj, w, dg[q], sg[q], sets[q], wts[q])
+            cert_o = tree_certified(tails, adj, w, do, so, sets[q], wts[q])
+            assert np.all(tie), (q, mism[~tie][:10])
+            assert cert_g.all() and cert_o.all(), (q, np.nonzero(~cert_g)[0][:10], np.nonzero(~cert_o)[0][:10])
+        print(f"MSAD set {q}: {len(sets[q])} sources, max relative difference {rel.max():.3e}, "
+              f"source-id differences {len(mism)} (all exact ties, certified)"
+              + (f", e.g. vertex {mism[0]}: source {sg[q][mism[0]]} vs {so[mism[0]]} "
+                 f"at {dg[q][mism[0]]!r}" if len(mism) else ""))

@@ -16,12 +16,14 @@ from oracle.refbind import CpuOracle, RefOracle, ref_available, rows_equal, REF_
 from svg_b200 import meshgen
 from tests.helpers import golden_params, load_golden, rows_from_padded, compare_rows
 
-REF_SRC = os.environ.get("SVG_REFERENCE_DIR", "/root/reference")
+# oracle/_ref is built by the package build step (__graft_entry__.build) where
+# the reference sources are checked out; SVG_REFERENCE_DIR names another copy.
+REF_SRC = os.environ.get("SVG_REFERENCE_DIR")
 
 
 @pytest.fixture(scope="module")
 def ref():
-    if not ref_available() and os.path.isdir(REF_SRC):
+    if not ref_available() and REF_SRC and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", ORACLE_DIR, "ref", "REF=" + REF_SRC], check=True)
     if not ref_available():
         pytest.skip("reference oracle not built (reference sources absent)")
