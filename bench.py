@@ -18,9 +18,11 @@ cpu_baseline / --impl reference
         the reference's own construction (its ICH compiled as host C++,
         oracle/_ref) over a seeded sample of sources on all host cores.
 
-Multi-GPU (--gpus N under torchrun): every rank builds its own replica of the
-workload (sources are independent; no data-path collective), scaling "weak";
-times are the max over ranks.
+Multi-GPU (--gpus N under torchrun): the build is sharded - every rank builds
+a contiguous range of the sources (sources are independent) and the CSR slices
+are all-gathered over NCCL so every rank holds the whole graph; scaling
+"strong", a step's time is the max over ranks of build + gather.  --replicas
+runs N whole builds instead (scaling "weak", no collective).
 """
 from __future__ import annotations
 
@@ -38,6 +40,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+from svg_b200.shard import gather_csr, shard_ranges  # noqa: E402
 
 WORKLOAD = dict(workload="svg_build_height_field_270x270_K500", mesh="height_field", grid=270, vertices=72900,
                 K=500, seed=1, mode="batched")
@@ -144,6 +148,31 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def device_view(ptr: int, n: int, typestr: str):
+    """A torch tensor over n elements of device memory the library owns (no copy)."""
+    import torch
+
+    class _Dev:
+        pass
+
+    d = _Dev()
+    d.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                  "version": 2, "strides": None}
+    return torch.as_tensor(d, device="cuda")
+
+
+def fma_rate():
+    """The GPU's measured FP64 fused-multiply-add rate (svg_device_fp64_rate), or None."""
+    try:
+        import svg_b200
+        x = C.c_double()
+        if svg_b200.lib().svg_device_fp64_rate(C.byref(x)) == 0:
+            return x.value
+    except Exception:
+        pass
+    return None
+
+
 def smi_index(local: int) -> str:
     """nvidia-smi's name for this process's GPU: the CUDA_VISIBLE_DEVICES entry
     (an index or a UUID) when that is set, else the local ordinal."""
@@ -171,37 +200,57 @@ def workload_mesh():
     return meshgen.height_field(WORKLOAD["grid"], seed=WORKLOAD["seed"])
 
 
-def roofline_figures(st: dict, peaks: dict) -> dict:
+def roofline_figures(st: dict, peaks: dict, fma_per_s: float | None = None) -> dict:
     """Roofline of the window-propagation kernel (k_ich_batched).
 
-    Algorithmic bytes per propagated window: 3 half-edge records of the
-    unfolded face (3 x 32 B), the apex and two opposite-vertex records
-    (3 x 16 B), four vertex-state probes (4 x 32 B), one split-state probe
-    (32 B), the window popped (16 B key + 48 B payload) and up to two pushed
-    (2 x 64 B): ~450 B; plus 24 B per exported candidate.  HBM-bound by
-    construction (no dense contraction); FP64 work ~300 flops per window.
-    """
+    HBM form, in the unit of the path's scope table: 250 algorithmic bytes per
+    propagated window (3 half-edge records of the unfolded face 60 B, 3
+    vertex-state reads 48 B, 1-2 split-state reads ~24 B, one 64 B window
+    written and read back 128 B) plus 12 B per output edge (adjacency +
+    length).  Beside it, the detailed count of what this kernel's loop reads
+    and writes per window: 3 half-edge records (3 x 32 B), the apex and two
+    opposite-vertex records (3 x 16 B), four vertex-state probes (4 x 32 B),
+    one split-state probe (32 B), the window popped (16 B key + 48 B payload)
+    and up to two pushed (2 x 64 B): ~450 B, plus 24 B per exported candidate.
+    FP64 form: ~300 FP64 operations per window (adds, multiplies, ~10
+    divides, ~12 square roots, no fused multiply-adds) against the measured
+    FP64 pipe rate (fused multiply-adds per second: one instruction each).
+    Traffic: ncu DRAM bytes per window of a captured launch
+    (profiles/ich_batched_traffic.json) x this launch's windows."""
     kernel_s = st["ms_ich"] / 1e3
-    bytes_alg = st["windows"] * 450.0 + st["edges"] * 24.0
-    achieved = bytes_alg / kernel_s / 1e9 if kernel_s > 0 else 0.0
     peak = peaks.get("hbm_gbs")
     src = "measured"
     if not peak:
         peak, src = 6650.0, "fallback"
+    bytes_alg = st["windows"] * 250.0 + st["edges"] * 12.0
+    bytes_det = st["windows"] * 450.0 + st["edges"] * 24.0
+    achieved = bytes_alg / kernel_s / 1e9 if kernel_s > 0 else 0.0
+    ach_det = bytes_det / kernel_s / 1e9 if kernel_s > 0 else 0.0
     traffic = None
+    tsrc = None
     tp = os.path.join(ROOT, "profiles", "ich_batched_traffic.json")
     if os.path.exists(tp):
         try:
             t = json.load(open(tp))
-            # scale the captured per-window traffic to this launch's windows
             traffic = t["dram_bytes_per_window"] * st["windows"]
+            tsrc = t.get("capture")
         except Exception:
             traffic = None
-    fp64 = st["windows"] * 300.0 / kernel_s / 1e12 if kernel_s > 0 else 0.0
+    ops = st["windows"] * 300.0
+    fp64 = {"ops_per_window": 300, "achieved_tflops": round(ops / kernel_s / 1e12, 4) if kernel_s > 0 else 0.0}
+    if fma_per_s:
+        fp64.update({"peak_fma_per_s": fma_per_s, "peak_tflops_fma_as_2": round(2 * fma_per_s / 1e12, 2),
+                     "frac_of_pipe": round(ops / kernel_s / fma_per_s, 5) if kernel_s > 0 else 0.0,
+                     "peak_source": "measured here (svg_device_fp64_rate: DFMA loop, CUDA events)"})
     return {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": src,
             "kernel": "k_ich_batched", "algorithmic_bytes_per_launch": bytes_alg,
-            "kernel_ms": st["ms_ich"], "fp64_tflops_est": round(fp64, 4)}
+            "unit_bytes": "250 B per window + 12 B per edge",
+            "detailed": {"bytes_per_launch": bytes_det, "achieved": round(ach_det, 2),
+                         "frac": round(ach_det / peak, 5), "unit_bytes": "450 B per window + 24 B per candidate"},
+            "traffic_source": tsrc,
+            "traffic_per_window": (traffic / st["windows"]) if traffic and st["windows"] else None,
+            "kernel_ms": st["ms_ich"], "fp64": fp64}
 
 
 def cpu_reference_run(pos, faces, K, budget_s: float, threads: int, seed: int = 0):
@@ -1013,6 +1062,8 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=400)
     ap.add_argument("--plain-seconds", type=float, default=30.0)
     ap.add_argument("--record", default="", help="also write the JSON line to this file")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: N whole builds (weak scaling) instead of one build sharded by source range")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -1053,14 +1104,45 @@ def main():
         flush.zero_()
         torch.cuda.synchronize()
 
-    def timed_build(mode=MODE_BATCHED):
+    # N > 1: every rank builds a contiguous source range and the CSR slices
+    # are all-gathered over NCCL (strong scaling); --replicas instead runs N
+    # whole builds (weak scaling, no collective)
+    shard = ws > 1 and not args.replicas
+    V = mesh.vertNum
+    sb, se = shard_ranges(V, ws)[rank] if shard else (0, V)
+
+    def gather_slices():
+        """Device time (ms) of the all-gather of this rank's CSR slice; every
+        rank ends up holding the whole graph."""
+        P = C.c_void_p
+        o, a, d = P(), P(), P()
+        L.svg_graph_device_csr(svg._g, C.byref(o), C.byref(a), C.byref(d))
+        nnz = svg.counts()[1]
+        off_t = device_view(o.value, V + 1, "<i8")
+        deg = (off_t[sb + 1:se + 1] - off_t[sb:se]).to(torch.int32)
+        adj_t = device_view(a.value, nnz, "<i4")
+        w_t = device_view(d.value, nnz, "<f8")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        gather_csr(dist, deg, adj_t, w_t, device="cuda")
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def timed_build(mode=MODE_BATCHED, sharded=shard):
         flush_l2()
         a = C.c_double()
         L.svg_timer_mark(C.byref(a))
-        st = svg.ConstructSVG(mode=mode)
+        if sharded:
+            st = svg.ConstructSVG(mode=mode, source_begin=sb, source_end=se)
+        else:
+            st = svg.ConstructSVG(mode=mode)
         b = C.c_double()
         L.svg_timer_mark(C.byref(b))
-        return b.value, st
+        ms = b.value
+        if sharded:
+            ms += gather_slices()
+        return ms, st
 
     for _ in range(args.warmup):
         timed_build()
@@ -1082,6 +1164,8 @@ def main():
     total_ms = sum(times)
     total_ms_max = max_over_ranks(dist, total_ms)
     value = replica_value(dist, float(edges), total_ms)
+    edges_per_build = sum_over_ranks(dist, float(st["edges"])) if shard else st["edges"]
+    windows_per_build = sum_over_ranks(dist, float(st["windows"])) if shard else st["windows"]
 
     # ---- end to end through the C ABI from host buffers: the step's inputs in
     # pinned host memory, the CSR read back into pinned host buffers allocated
@@ -1107,7 +1191,7 @@ def main():
         s2 = SVG()
         s2.AssignMesh(m2)
         s2.SetParameters(K_BUILD, 10, 2)
-        st2 = s2.ConstructSVG()
+        st2 = s2.ConstructSVG(source_begin=sb, source_end=se) if shard else s2.ConstructSVG()
         off, adj, dist_h = s2.csr(out=out_bufs)
         b = C.c_double()
         L.svg_timer_mark(C.byref(b))
@@ -1130,11 +1214,10 @@ def main():
             peaks = json.load(open(pp))
         plain = None
         if not args.no_plain:
-            ms_p, stp = timed_build(MODE_PLAIN)
+            ms_p, stp = timed_build(MODE_PLAIN, sharded=False)
             plain = {"build_ms": ms_p, "edges_per_s": stp["edges"] / (ms_p / 1e3),
-                     "speedup_batched_vs_plain": (ms_p / (total_ms / args.steps)), "grid": "64x128",
-                     "windows": stp["windows"]}
-            svg.ConstructSVG(mode=MODE_BATCHED)  # leave the batched graph resident
+                     "speedup_batched_vs_plain": (ms_p / (total_ms_max / args.steps)), "grid": "64x128",
+                     "windows": stp["windows"], "gpus": 1}
         cpu = None
         if not args.no_cpu:
             try:
@@ -1145,12 +1228,17 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(WORKLOAD, l2="flushed between steps (256 MiB write)", parallelism=f"replicas{ws}",
-                           edges_per_build=st["edges"], windows_per_build=st["windows"]),
+            "scaling": "strong" if shard else "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, l2="flushed between steps (256 MiB write)",
+                           parallelism=(f"shard{ws}: contiguous source ranges, CSR slices all-gathered over NCCL"
+                                        if shard else f"replicas{ws}"),
+                           edges_per_build=edges_per_build, windows_per_build=windows_per_build,
+                           work_order="timed steps: heaviest sources first for two waves (per-source costs "
+                                      "recorded by the warm-up builds), then vertex order; e2e: a fresh mesh "
+                                      "every step, ordered by a K/10 probe build inside the timed region"),
             "build_s": total_ms_max / args.steps / 1e3,
             "kernel_ms_per_step": statistics.mean(kern),
-            "roofline": roofline_figures(st, peaks),
+            "roofline": roofline_figures(st, peaks, fma_rate()),
             "cpu_baseline": cpu,
             "plain": plain,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -101,6 +101,10 @@ typedef struct svg_build_opts {
     int64_t hbm_budget;       /* bytes of scratch the build may hold (0 = automatic) */
     int32_t source_begin;     /* build rows for sources [source_begin, source_end) only; */
     int32_t source_end;       /* 0,0 = all vertices */
+    int32_t coop_sources;     /* batched, with a heaviest-first order: this many of the heaviest sources are
+                                 each run by a whole warp (warp-cooperative heap and table operations), the
+                                 rest one per lane; -1 automatic, 0 none */
+    int32_t coop_warps;       /* warps that run them (0 automatic) */
 } svg_build_opts;
 
 typedef struct svg_build_stats {
@@ -122,6 +126,8 @@ typedef struct svg_build_stats {
     int32_t retried_sources;  /* sources re-run with larger scratch tables */
     int32_t launches;         /* kernels launched */
     int64_t scratch_bytes;    /* device scratch held by the build */
+    int32_t coop_sources;     /* sources run by whole warps */
+    int32_t coop_warps;       /* warps that ran them */
 } svg_build_stats;
 
 void svg_build_opts_default(svg_build_opts* o);
@@ -184,6 +190,24 @@ svg_status svg_sssd_batch(svg_graph* g, int32_t n, const int32_t* s, const int32
 svg_status svg_msad_batch(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs,
                           const double* weights, double* dist, int32_t* src_id);
 
+/* SVG::SolveMSAD with SVG::GraphDistInfo::pathParentIndex (SVG.cu:396):
+ * as svg_msad_batch, plus parent[q*nv + v] = the vertex before v on a
+ * shortest path of set q (-1 for a source that kept its own label and for
+ * unreached vertices).  Where several predecessors give the same distance,
+ * the smallest vertex id is named (the reference names the first its heap
+ * relaxes from).  src_id may be NULL.  Host buffers. */
+svg_status svg_msad_batch_paths(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs,
+                                const double* weights, double* dist, int32_t* src_id, int32_t* parent);
+
+/* SVG::SolveSSSD followed by the reference driver's walk along
+ * pathParentIndex from t back to s (kernel.cu:75-82): path[0] = t, ...,
+ * path[len-1] = s, path_dist (optional) the distance of each from s; *dist
+ * (optional) the s-t distance.  An unreachable t gives len 0 and DBL_MAX.
+ * A path longer than cap returns SVG_ERR_ARG with the needed length in *len.
+ * Runs a full search from s (device); for many pairs use svg_sssd_batch. */
+svg_status svg_sssd_path(svg_graph* g, int32_t s, int32_t t, int32_t cap, int32_t* path, double* path_dist,
+                         int32_t* len, double* dist);
+
 /* Same queries on device-resident inputs/outputs (no host copies). */
 svg_status svg_sssd_batch_device(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t,
                                  double* d_dist);
@@ -197,21 +221,30 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
  * to an outer framework's pool, or that runs where a cudaMalloc would
  * synchronise the device or break a capture.  The caller provides every
  * buffer; the kernel's scratch is a fixed array inside the library (about
- * 15 MiB per GPU that loads the library, held until the library unloads).
+ * 19 MiB per GPU that loads the library, held until the library unloads),
+ * with tables sized as svg_build's first pass sizes them at K = 128.
  *   m            a mesh already on the device (svg_mesh_upload, which does
  *                allocate, must have been called earlier)
  *   K            1..128 (queue capacities are the reference's 1023)
  *   [source_begin, source_end)  sources to build, row r = source_begin + r
- *   d_tails      device int32[n]: row length, or -1 if that source outgrew
- *                the fixed tables
+ *   d_tails      device int32[n]: row length, or a code:
+ *                  -1  the source outgrew the fixed tables (svg_build re-runs
+ *                      such a source with larger tables);
+ *                  -2  an iteration cap stopped the source, or it reached a
+ *                      step the reference leaves undefined (svg_build flags
+ *                      both in svg_graph_source_stats); the row is not written.
+ *                A source where the reference's own fixed hash tables would
+ *                overflow gets the same row as svg_build gives it (the exact
+ *                ICH's), and is not flagged here.
  *   d_adj, d_dist  device int32[n*K], double[n*K]: padded rows, the same
  *                neighbours and lengths as svg_build's rows
  *   stream       cudaStream_t (NULL: the legacy default stream)
  * Asynchronous: outputs are complete when the stream reaches this point.
  * All calls share the one scratch array, so calls whose kernels could run
- * at the same time on the GPU race; serialise them.  The first call on each
- * device looks up the array's device address; make that first call before
- * any stream capture. */
+ * at the same time on the GPU race; serialise them.  Every call looks up the
+ * array's device address on the current device (no allocation); the first
+ * call on a device also loads the library's kernels there, so make that
+ * first call before any stream capture. */
 svg_status svg_build_rows_static(svg_mesh* m, int32_t K, int32_t source_begin, int32_t source_end,
                                  int32_t* d_tails, int32_t* d_adj, double* d_dist, void* stream);
 
@@ -301,6 +334,13 @@ size_t svg_trim_device_cache(void);
  * of that since the last reset, and cached for reuse.  reset_peak != 0 sets
  * the high-water mark to the current use.  No counterpart in the reference. */
 void svg_device_memory(int64_t* in_use, int64_t* peak, int64_t* cached, int32_t reset_peak);
+
+/* Measured FP64 pipe rate of the current GPU: fused multiply-adds per second
+ * of a kernel that keeps every SM's FP64 units busy (CUDA events, ~0.1 s).
+ * The denominator of the build kernel's FP64 roofline (each of its FP64 adds,
+ * multiplies, divides and square roots issues on the same pipe).  No
+ * counterpart in the reference. */
+svg_status svg_device_fp64_rate(double* fma_per_s);
 
 /* Synchronise the library's stream; returns the device time in ms since the
  * previous svg_timer_mark (CUDA events on the library stream). */

@@ -55,6 +55,7 @@ class BuildOptions(C.Structure):
         ("threads_per_block", C.c_int32), ("blocks", C.c_int32), ("with_paths", C.c_int32),
         ("heavy_first", C.c_int32), ("hbm_budget", C.c_int64),
         ("source_begin", C.c_int32), ("source_end", C.c_int32),
+        ("coop_sources", C.c_int32), ("coop_warps", C.c_int32),
     ]
 
 
@@ -66,7 +67,7 @@ class BuildStats(C.Structure):
         ("max_pseudo_queue", C.c_int32), ("queue_drop_sources", C.c_int32),
         ("ref_overflow_sources", C.c_int32), ("watchdog_sources", C.c_int32),
         ("undefined_sources", C.c_int32), ("retried_sources", C.c_int32), ("launches", C.c_int32),
-        ("scratch_bytes", C.c_int64),
+        ("scratch_bytes", C.c_int64), ("coop_sources", C.c_int32), ("coop_warps", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -108,6 +109,7 @@ EXPORTS = [
     "svg_server_submit_build", "svg_server_submit_sssd", "svg_server_submit_msad", "svg_server_wait",
     "svg_server_poll", "svg_server_take", "svg_server_stats", "svg_server_submit_msad_into",
     "svg_device_memory", "svg_graph_set_query_form", "svg_server_resident",
+    "svg_msad_batch_paths", "svg_sssd_path", "svg_device_fp64_rate",
 ]
 
 _lib = None
@@ -145,9 +147,13 @@ def lib() -> C.CDLL:
     L.svg_graph_load.argtypes = [_P, C.c_int32, C.c_char_p, C.POINTER(_P)]
     L.svg_sssd_batch.argtypes = [_P, C.c_int32, _i32p, _i32p, _f64p]
     L.svg_msad_batch.argtypes = [_P, C.c_int32, _i64p, _P, _P, _f64p, _P]
+    L.svg_msad_batch_paths.argtypes = [_P, C.c_int32, _i64p, _P, _P, _f64p, _P, _P]
+    L.svg_sssd_path.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, C.POINTER(C.c_int32),
+                                C.POINTER(C.c_double)]
     L.svg_sssd_batch_device.argtypes = [_P, C.c_int32, _P, _P, _P]
     L.svg_msad_batch_device.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P]
     L.svg_timer_mark.argtypes = [C.POINTER(C.c_double)]
+    L.svg_device_fp64_rate.argtypes = [C.POINTER(C.c_double)]
     L.svg_build_rows_static.argtypes = [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P]
     L.svg_trim_device_cache.restype = C.c_size_t
     L.svg_server_opts_default.argtypes = [C.POINTER(ServerOptions)]
@@ -363,6 +369,32 @@ class SVG:
                                     sid.ctypes.data_as(_P) if with_src else None))
         dist = dist.reshape(n, V)
         return (dist, sid.reshape(n, V)) if with_src else dist
+
+    def msad_paths(self, sets, weights=None):
+        """msad_batch plus parent pointers (pathParentIndex): (dist, src, parent), each (n, V)."""
+        V = self.mesh.vertNum
+        n = len(sets)
+        off = np.zeros(n + 1, np.int64)
+        np.cumsum([len(x) for x in sets], out=off[1:])
+        srcs = np.ascontiguousarray(np.concatenate(sets) if n else np.zeros(0), np.int32)
+        w = np.zeros(len(srcs)) if weights is None else \
+            np.ascontiguousarray(np.concatenate(weights) if n else np.zeros(0), np.float64)
+        dist = np.zeros(n * V)
+        sid = np.zeros(n * V, np.int32)
+        par = np.zeros(n * V, np.int32)
+        _check(lib().svg_msad_batch_paths(self._g, n, off, srcs.ctypes.data_as(_P), w.ctypes.data_as(_P), dist,
+                                          sid.ctypes.data_as(_P), par.ctypes.data_as(_P)))
+        return dist.reshape(n, V), sid.reshape(n, V), par.reshape(n, V)
+
+    def sssd_path(self, s: int, t: int, cap: int = 1 << 16):
+        """(vertices t ... s along pathParentIndex, their distances from s, the s-t distance)."""
+        path = np.zeros(cap, np.int32)
+        pd = np.zeros(cap)
+        n = C.c_int32()
+        d = C.c_double()
+        _check(lib().svg_sssd_path(self._g, int(s), int(t), cap, path.ctypes.data_as(_P), pd.ctypes.data_as(_P),
+                                   C.byref(n), C.byref(d)))
+        return path[:n.value].copy(), pd[:n.value].copy(), d.value
 
     def SolveMSAD(self, sources, sourceWeights):
         d, s = self.msad_batch([np.asarray(sources)], [np.asarray(sourceWeights, np.float64)])

@@ -183,6 +183,23 @@ void free_graph_device(svg_graph* g) {
     g->qdefault = nullptr;
 }
 
+// FP64 pipe rate: every thread runs 8 independent chains of fused
+// multiply-adds (explicit __fma_rn: the library is built with --fmad=false),
+// so the pipe, not latency, bounds it.
+__global__ void k_dfma_rate(double* out, int iters, double b, double c) {
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = (double)(threadIdx.x + j) * 1e-3;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = __fma_rn(a[j], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += a[j];
+    if (s == 12345.678) out[0] = s;  // keeps the chains live; never true for these inputs
+}
+
 }  // namespace svgb
 
 using namespace svgb;
@@ -306,6 +323,7 @@ void svg_build_opts_default(svg_build_opts* o) {
     o->mode = SVG_BUILD_BATCHED;
     o->with_paths = 1;
     o->heavy_first = 1;
+    o->coop_sources = -1;
 }
 
 svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out) {
@@ -571,41 +589,96 @@ svg_status svg_sssd_batch(svg_graph* g, int32_t n, const int32_t* s, const int32
     });
 }
 
+}  // extern "C"
+
+namespace {
+// svg_msad_batch and svg_msad_batch_paths: host buffers in and out; parent
+// pointers (optional) from the finished distances on the device.
+svg_status msad_host(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs, const double* weights,
+                     double* dist, int32_t* src_id, int32_t* parent) {
+    if (!g || n < 0 || (n > 0 && (!set_offsets || !dist))) throw SvgError{SVG_ERR_ARG, "bad argument"};
+    if (n == 0) return SVG_OK;
+    int64_t total = set_offsets[n];
+    if (set_offsets[0] != 0 || total < 0) throw SvgError{SVG_ERR_ARG, "set_offsets must start at 0"};
+    for (int32_t q = 0; q < n; ++q)
+        if (set_offsets[q + 1] < set_offsets[q]) throw SvgError{SVG_ERR_ARG, "set_offsets not monotone"};
+    if (total > 0 && (!srcs || !weights)) throw SvgError{SVG_ERR_ARG, "null sources"};
+    for (int64_t i = 0; i < total; ++i)
+        if (srcs[i] < 0 || srcs[i] >= g->nv) throw SvgError{SVG_ERR_ARG, "source vertex out of range"};
+    cudaStream_t st = lib_stream();
+    DevBuf b;
+    const bool want_src = src_id || parent;  // a source keeps parent -1 only where it kept its own label
+    size_t ob = sizeof(int64_t) * ((size_t)n + 1), sb = sizeof(int32_t) * (size_t)std::max<int64_t>(total, 1),
+           wb = sizeof(double) * (size_t)std::max<int64_t>(total, 1), db = sizeof(double) * (size_t)n * g->nv,
+           ib = want_src ? sizeof(int32_t) * (size_t)n * g->nv : 0, pb = parent ? sizeof(int32_t) * (size_t)n * g->nv : 0;
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    b.reserve(al(ob) + al(sb) + al(wb) + al(db) + al(ib) + al(pb) + 256);
+    char* p = b.as<char>();
+    int64_t* doff = reinterpret_cast<int64_t*>(p); p += al(ob);
+    int32_t* dsrc = reinterpret_cast<int32_t*>(p); p += al(sb);
+    double* dw = reinterpret_cast<double*>(p); p += al(wb);
+    double* dd = reinterpret_cast<double*>(p); p += al(db);
+    int32_t* did = want_src ? reinterpret_cast<int32_t*>(p) : nullptr; p += al(ib);
+    int32_t* dpar = parent ? reinterpret_cast<int32_t*>(p) : nullptr;
+    SVG_CUDA(cudaMemcpyAsync(doff, set_offsets, ob, cudaMemcpyHostToDevice, st));
+    if (total > 0) {
+        SVG_CUDA(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * total, cudaMemcpyHostToDevice, st));
+        SVG_CUDA(cudaMemcpyAsync(dw, weights, sizeof(double) * total, cudaMemcpyHostToDevice, st));
+    }
+    svg_status r = run_msad(g, n, doff, dsrc, dw, dd, did, total);
+    if (r != SVG_OK) return r;
+    if (dpar) query_parents(g, n, dd, did, dpar, st);
+    SVG_CUDA(cudaMemcpyAsync(dist, dd, db, cudaMemcpyDeviceToHost, st));
+    if (src_id) SVG_CUDA(cudaMemcpyAsync(src_id, did, ib, cudaMemcpyDeviceToHost, st));
+    if (parent) SVG_CUDA(cudaMemcpyAsync(parent, dpar, pb, cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    return SVG_OK;
+}
+}  // namespace
+
+extern "C" {
+
 svg_status svg_msad_batch(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs,
                           const double* weights, double* dist, int32_t* src_id) {
+    return guarded([&]() -> svg_status { return msad_host(g, n, set_offsets, srcs, weights, dist, src_id, nullptr); });
+}
+
+svg_status svg_msad_batch_paths(svg_graph* g, int32_t n, const int64_t* set_offsets, const int32_t* srcs,
+                                const double* weights, double* dist, int32_t* src_id, int32_t* parent) {
     return guarded([&]() -> svg_status {
-        if (!g || n < 0 || (n > 0 && (!set_offsets || !dist))) throw SvgError{SVG_ERR_ARG, "bad argument"};
-        if (n == 0) return SVG_OK;
-        int64_t total = set_offsets[n];
-        if (set_offsets[0] != 0 || total < 0) throw SvgError{SVG_ERR_ARG, "set_offsets must start at 0"};
-        for (int32_t q = 0; q < n; ++q)
-            if (set_offsets[q + 1] < set_offsets[q]) throw SvgError{SVG_ERR_ARG, "set_offsets not monotone"};
-        if (total > 0 && (!srcs || !weights)) throw SvgError{SVG_ERR_ARG, "null sources"};
-        for (int64_t i = 0; i < total; ++i)
-            if (srcs[i] < 0 || srcs[i] >= g->nv) throw SvgError{SVG_ERR_ARG, "source vertex out of range"};
-        cudaStream_t st = lib_stream();
-        DevBuf b;
-        size_t ob = sizeof(int64_t) * ((size_t)n + 1), sb = sizeof(int32_t) * (size_t)std::max<int64_t>(total, 1),
-               wb = sizeof(double) * (size_t)std::max<int64_t>(total, 1), db = sizeof(double) * (size_t)n * g->nv,
-               ib = src_id ? sizeof(int32_t) * (size_t)n * g->nv : 0;
-        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-        b.reserve(al(ob) + al(sb) + al(wb) + al(db) + al(ib) + 256);
-        char* p = b.as<char>();
-        int64_t* doff = reinterpret_cast<int64_t*>(p); p += al(ob);
-        int32_t* dsrc = reinterpret_cast<int32_t*>(p); p += al(sb);
-        double* dw = reinterpret_cast<double*>(p); p += al(wb);
-        double* dd = reinterpret_cast<double*>(p); p += al(db);
-        int32_t* did = src_id ? reinterpret_cast<int32_t*>(p) : nullptr;
-        SVG_CUDA(cudaMemcpyAsync(doff, set_offsets, ob, cudaMemcpyHostToDevice, st));
-        if (total > 0) {
-            SVG_CUDA(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * total, cudaMemcpyHostToDevice, st));
-            SVG_CUDA(cudaMemcpyAsync(dw, weights, sizeof(double) * total, cudaMemcpyHostToDevice, st));
-        }
-        svg_status r = run_msad(g, n, doff, dsrc, dw, dd, did, total);
+        if (!parent) throw SvgError{SVG_ERR_ARG, "parent buffer is null"};
+        return msad_host(g, n, set_offsets, srcs, weights, dist, src_id, parent);
+    });
+}
+
+svg_status svg_sssd_path(svg_graph* g, int32_t s, int32_t t, int32_t cap, int32_t* path, double* path_dist,
+                         int32_t* len, double* dist) {
+    return guarded([&]() -> svg_status {
+        if (!g || !len || cap < 0 || (cap > 0 && !path)) throw SvgError{SVG_ERR_ARG, "bad argument"};
+        if (s < 0 || s >= g->nv || t < 0 || t >= g->nv) throw SvgError{SVG_ERR_ARG, "query vertex out of range"};
+        const size_t V = (size_t)g->nv;
+        std::vector<double> d(V);
+        std::vector<int32_t> par(V);
+        const int64_t off[2] = {0, 1};
+        const double w0 = 0.0;
+        svg_status r = msad_host(g, 1, off, &s, &w0, d.data(), nullptr, par.data());
         if (r != SVG_OK) return r;
-        SVG_CUDA(cudaMemcpyAsync(dist, dd, db, cudaMemcpyDeviceToHost, st));
-        if (src_id) SVG_CUDA(cudaMemcpyAsync(src_id, did, ib, cudaMemcpyDeviceToHost, st));
-        SVG_CUDA(cudaStreamSynchronize(st));
+        if (dist) *dist = d[(size_t)t];
+        *len = 0;
+        if (!(d[(size_t)t] < DBL_MAX)) return SVG_OK;  // unreachable: empty path
+        if (d[(size_t)t] < 0.0) throw SvgError{SVG_ERR_NOMEM, "the search exceeded its round limit"};
+        int32_t n = 0;
+        for (int32_t v = t;; v = par[(size_t)v]) {
+            if (v < 0 || n > g->nv) throw SvgError{SVG_ERR_STATE, "parent chain does not reach the source"};
+            if (n < cap) {
+                path[n] = v;
+                if (path_dist) path_dist[n] = d[(size_t)v];
+            }
+            ++n;
+            if (v == s) break;
+        }
+        *len = n;
+        if (n > cap) throw SvgError{SVG_ERR_ARG, "path has " + std::to_string(n) + " vertices, cap " + std::to_string(cap)};
         return SVG_OK;
     });
 }
@@ -618,6 +691,34 @@ void svg_device_memory(int64_t* in_use, int64_t* peak, int64_t* cached, int32_t 
     if (in_use) *in_use = (int64_t)a;
     if (peak) *peak = (int64_t)b;
     if (cached) *cached = (int64_t)c;
+}
+
+svg_status svg_device_fp64_rate(double* fma_per_s) {
+    return guarded([&]() -> svg_status {
+        if (!fma_per_s) throw SvgError{SVG_ERR_ARG, "null argument"};
+        int dev = 0, sms = 0;
+        SVG_CUDA(cudaGetDevice(&dev));
+        SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        cudaStream_t st = lib_stream();
+        double* d = dev_alloc_n<double>(1);
+        const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+        cudaEvent_t e0, e1;
+        SVG_CUDA(cudaEventCreate(&e0));
+        SVG_CUDA(cudaEventCreate(&e1));
+        k_dfma_rate<<<blocks, threads, 0, st>>>(d, 256, 0.999999, 1e-7);  // warm-up
+        SVG_CUDA(cudaEventRecord(e0, st));
+        k_dfma_rate<<<blocks, threads, 0, st>>>(d, iters, 0.999999, 1e-7);
+        SVG_CUDA(cudaEventRecord(e1, st));
+        SVG_CUDA(cudaEventSynchronize(e1));
+        SVG_CUDA(cudaGetLastError());
+        float ms = 0.f;
+        SVG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        dev_free(d);
+        *fma_per_s = (double)blocks * threads * 8.0 * iters / (ms / 1e3);
+        return SVG_OK;
+    });
 }
 
 svg_status svg_timer_mark(double* ms_since_last) {

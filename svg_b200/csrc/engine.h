@@ -126,6 +126,9 @@ int query_slots_per_sm();            // plain form: query blocks resident per SM
 int query_cluster_size();            // cluster form: blocks per query
 int query_cluster_slots(int csize);  // cluster form: clusters resident at once
 void qctx_free(svg_qctx* c);
+// parent pointers of n finished MSAD searches on the device (d_src may be null)
+void query_parents(svg_graph* g, int32_t n, const double* d_dist, const int32_t* d_src, int32_t* d_parent,
+                   cudaStream_t st);
 void qctx_sssd(svg_qctx* c, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist, cudaStream_t st);
 void qctx_msad(svg_qctx* c, int32_t n, const int64_t* d_off, const int32_t* d_src, const double* d_w, double* d_dist,
                int32_t* d_src_id, cudaStream_t st);

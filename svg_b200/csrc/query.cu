@@ -18,6 +18,7 @@
 // reference's consistent heuristic no unsettled path can then be shorter.
 // Per-slot stamp arrays replace clearing: a stamp is never reused.
 #include <cfloat>
+#include <climits>
 
 #include <cooperative_groups.h>
 
@@ -689,7 +690,66 @@ __global__ void k_fill(unsigned long long* p, size_t n, unsigned long long v) {
 
 size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 
+__global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// Parent pointers of n finished searches (SVG::GraphDistInfo::pathParentIndex,
+// SVG.cu:396): parent[q*nv + v] = the smallest u with an edge u -> v such that
+// dist[u] + w == dist[v] (the addition the searches relax with) and
+// dist[u] < dist[v].  Every vertex a search reached except its sources has
+// such an edge: the relaxation that left dist[v] final read some dist[u], and
+// had dist[u] fallen after it, v would have been relaxed again.  The strict
+// dist[u] < dist[v] keeps the pointers acyclic.  One warp per (query, row u);
+// parent must hold INT_MAX on entry.
+__global__ void k_parents(const int64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                          const double* __restrict__ w, int32_t nv, int32_t n, const double* __restrict__ dist,
+                          int32_t* __restrict__ parent) {
+    const int lane = threadIdx.x & 31;
+    const int64_t rows = (int64_t)n * nv;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
+        const int64_t q = r / nv;
+        const int u = (int)(r - q * nv);
+        const double* d = dist + q * nv;
+        const double du = d[u];
+        if (!(du < DBL_MAX)) continue;
+        const int64_t e1 = __ldg(&off[u + 1]);
+        for (int64_t e = __ldg(&off[u]) + lane; e < e1; e += 32) {
+            const int v = __ldg(&adj[e]);
+            const double dv = d[v];
+            if (du < dv && du + __ldg(&w[e]) == dv) atomicMin(&parent[q * nv + v], u);
+        }
+    }
+}
+
+// INT_MAX (no parent edge) -> -1; a vertex that kept its own source label
+// (src[v] == v) is a root, as the reference leaves a source's parent at -1.
+__global__ void k_parents_finish(int32_t* parent, const int32_t* src, int32_t nv, int64_t total) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int v = (int)(i % nv);
+        if (parent[i] == INT_MAX || (src && src[i] == v)) parent[i] = -1;
+    }
+}
+
 }  // namespace
+
+void query_parents(svg_graph* g, int32_t n, const double* d_dist, const int32_t* d_src, int32_t* d_parent,
+                   cudaStream_t st) {
+    if (n <= 0 || g->nv <= 0) return;
+    const int64_t total = (int64_t)n * g->nv;
+    k_fill_i32<<<256, 256, 0, st>>>(d_parent, total, INT_MAX);
+    int dev = 0, sms = 0;
+    SVG_CUDA(cudaGetDevice(&dev));
+    SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t want = (total + 7) / 8;  // blocks of 8 warps
+    k_parents<<<(int)std::min<int64_t>(want, (int64_t)sms * 16), 256, 0, st>>>(g->off, g->adj, g->dist, g->nv, n,
+                                                                               d_dist, d_parent);
+    k_parents_finish<<<(int)std::min<int64_t>((total + 255) / 256, (int64_t)sms * 16), 256, 0, st>>>(
+        d_parent, d_src, g->nv, total);
+    SVG_CUDA(cudaGetLastError());
+}
 
 // Bucket width of the near-far search: the mean SVG edge length, computed once per graph.
 double graph_delta(svg_graph* g, cudaStream_t st) {

@@ -93,26 +93,3 @@ def first_row_mismatches(off_a, nodes_a, off_b, nodes_b,
             rows = np.unique(row_of[diff])[:limit]
             out += [(int(r), f) for r in rows]
     return out[:limit]
-
-
-def tree_certified(tails, adj, w, dist, src, sources, weights):
-    """Local certificate of a multi-source shortest-path labelling: every
-    reached vertex v is a source carrying its own id and weight, or has an
-    in-edge (u -> v) with dist[u] + w == dist[v] and src[u] == src[v].  Edge
-    weights are positive, so following such edges back ends at the source
-    src[v]: that source's tree reaches v at exactly dist[v].  Returns the
-    boolean array of certified vertices (unreached vertices count as certified).
-    tails[i] is the row (tail vertex) of CSR edge i."""
-    V = len(dist)
-    u = tails
-    ok_edge = (dist[u] + w == dist[adj]) & (src[u] == src[adj]) & (dist[u] < np.finfo(np.float64).max)
-    cert = np.zeros(V, bool)
-    cert[adj[ok_edge]] = True
-    last_w = {}
-    for s_, w_ in zip(sources, weights):
-        last_w[int(s_)] = float(w_)  # a repeated source keeps its last weight
-    for s_, w_ in last_w.items():
-        if src[s_] == s_ and dist[s_] == w_:
-            cert[s_] = True
-    cert |= dist == np.finfo(np.float64).max
-    return cert

@@ -28,7 +28,7 @@ import pytest
 from oracle.refbind import CpuOracle, RefOracle, ref_available
 from svg_b200 import MODE_BATCHED, MODE_PLAIN, SVG, Mesh, meshgen
 from svg_b200.build_ext import build as build_lib
-from tests.helpers import csr_from_padded, first_row_mismatches, tree_certified
+from tests.helpers import csr_from_padded, first_row_mismatches
 
 pytestmark = pytest.mark.gpu
 
@@ -190,18 +190,39 @@ def test_queries_on_large_torus_graph_match_oracle(torus750k):
 
     with ThreadPoolExecutor(min(CORES, len(sets))) as ex:
         outs = list(ex.map(oracle_msad, range(len(sets))))
-    tails = np.repeat(np.arange(V, dtype=np.int32), np.diff(off))  # edge -> its row (tail vertex)
     for q, (do, so, _) in enumerate(outs):
         rel = np.abs(dg[q] - do) / np.maximum(do, 1e-300)
         assert np.all(rel <= 1e-8), (q, rel.max())
         mism = np.nonzero(sg[q] != so)[0]
-        if len(mism):
-            tie = np.abs(dg[q][mism] - do[mism]) <= 1e-12 * do[mism]
-            cert_g = tree_certified(tails, adj, w, dg[q], sg[q], sets[q], wts[q])
-            cert_o = tree_certified(tails, adj, w, do, so, sets[q], wts[q])
-            assert np.all(tie), (q, mism[~tie][:10])
-            assert cert_g.all() and cert_o.all(), (q, np.nonzero(~cert_g)[0][:10], np.nonzero(~cert_o)[0][:10])
+        checked = _certify_ties(cm, off, adj, w, sets[q], wts[q], dg[q], sg[q], mism)
         print(f"MSAD set {q}: {len(sets[q])} sources, max relative difference {rel.max():.3e}, "
-              f"source-id differences {len(mism)} (all exact ties, certified)"
-              + (f", e.g. vertex {mism[0]}: source {sg[q][mism[0]]} vs {so[mism[0]]} "
-                 f"at {dg[q][mism[0]]!r}" if len(mism) else ""))
+              f"source-id differences {len(mism)} (ties; {checked} checked against the named source's own "
+              f"distance)" + (f", e.g. vertex {mism[0]}: source {sg[q][mism[0]]} vs the oracle's {so[mism[0]]} "
+                              f"at {dg[q][mism[0]]!r}" if len(mism) else ""))
+
+
+def _certify_ties(cm, off, adj, w, srcs, wts, dg, sg, mism, max_sources=256):
+    """Each vertex v where the GPU names another source a than the oracle must
+    be an exact tie: a's own tree (the oracle's Dijkstra from a alone, seeded
+    with a's weight) reaches v within 1e-12 relative of v's distance.  Checked
+    for up to `max_sources` distinct sources (a seeded sample beyond that)."""
+    if len(mism) == 0:
+        return 0
+    last_w = {}
+    for s_, w_ in zip(srcs, wts):
+        last_w[int(s_)] = float(w_)  # a repeated source keeps its last weight
+    named = np.unique(sg[mism])
+    if len(named) > max_sources:
+        named = np.sort(np.random.default_rng(7).choice(named, max_sources, replace=False))
+
+    def one(a):
+        da, _, _ = cm.msad(off, adj, w, np.array([a], np.int32), np.array([last_w[int(a)]]))
+        vs = mism[sg[mism] == a]
+        return vs, da[vs]
+
+    n = 0
+    with ThreadPoolExecutor(min(CORES, len(named))) as ex:
+        for vs, da in ex.map(one, named):
+            assert np.all(np.abs(da - dg[vs]) <= 1e-12 * dg[vs]), (vs[:5], da[:5], dg[vs][:5])
+            n += len(vs)
+    return n
