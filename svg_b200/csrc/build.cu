@@ -22,7 +22,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 
 #include "engine.h"
 #include "ich.cuh"
@@ -946,13 +945,14 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
 //
 // Limits: kStaticLanes = 128 lanes (one source each at a time, grid-stride
 // over the range), K <= kStaticMaxK = 128, queue capacities fixed at the
-// reference's 1023, tables sized for K = 128.  The array takes
-// kStaticScratchBytes (about 15 MiB) on every GPU that loads the library, for
-// as long as the library stays loaded.  All calls share it: two calls whose
-// kernels overlap on the GPU (different streams, or different host threads)
-// race on it and produce garbage; serialise them.  Each source resets its own
-// tables before it starts, so nothing carried over from an earlier call is
-// ever read and the array never needs clearing.
+// reference's 1023, tables sized as the regular build's first pass sizes them
+// at K = 128 (1,024 vertex slots taking 768 keys, 1,024 split slots taking
+// 768 keys).  The array takes kStaticScratchBytes (about 19 MiB) on every GPU
+// that loads the library, for as long as the library stays loaded.  All calls
+// share it: two calls whose kernels overlap on the GPU (different streams, or
+// different host threads) race on it and produce garbage; serialise them.
+// Each source resets its own tables before it starts, so nothing carried over
+// from an earlier call is ever read and the array never needs clearing.
 // ---------------------------------------------------------------------------
 namespace svgb {
 namespace {
@@ -961,10 +961,13 @@ constexpr int kStaticLanes = 128;
 constexpr int kStaticMaxK = 128;
 constexpr int kStaticWcap = 1023;
 constexpr int kStaticPcap = 1023;
-constexpr int kStaticVcapLog2 = 9;  // 512 slots >= 2 * (2*128 + 1)
-constexpr int kStaticScapLog2 = 9;  // 512 slots >= 4 * 128
-constexpr int kStaticVlimit = 384;
-constexpr int kStaticSlimit = 384;
+// The regular build's first-pass sizing at K = 128: vertex slots
+// 2^ceil(log2(2 * (2K + 1))) = 1024, split slots 2^ceil(log2(8K)) = 1024 (split
+// keys reach about 1.6x the vertices reached), each filled to 3/4 at most.
+constexpr int kStaticVcapLog2 = 10;
+constexpr int kStaticScapLog2 = 10;
+constexpr int kStaticVlimit = 768;
+constexpr int kStaticSlimit = 768;
 
 constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 constexpr int kStaticStride = (kStaticWcap + 4 + 3) / 4 * 4;  // heap entries per lane
@@ -981,29 +984,21 @@ constexpr size_t kStaticScratchBytes =
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-// Device address of g_static_scratch, resolved once per device.  In host code
-// the array's name is only a host-side stand-in for the symbol, never a
-// device address.
-constexpr int kMaxDevices = 64;
-void* g_static_ptr[kMaxDevices] = {nullptr};
-std::mutex g_static_mu;
-
+// Device address of g_static_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in for the symbol, never a device
+// address.  The lookup runs on every call (it allocates nothing and costs
+// microseconds), so a context re-created after cudaDeviceReset, which loads
+// the module and its array anew, is never handed a stale address.  On a
+// device's first call it also loads the library's kernels there.
 void* static_scratch_address() {
-    int dev = 0;
-    SVG_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) throw SvgError{SVG_ERR_ARG, "device ordinal out of range"};
-    std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess || p == nullptr) {
-            cudaGetLastError();
-            throw SvgError{SVG_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch) failed: ") +
-                                             cudaGetErrorString(e)};
-        }
-        g_static_ptr[dev] = p;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        throw SvgError{SVG_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch) failed: ") +
+                                         cudaGetErrorString(e)};
     }
-    return g_static_ptr[dev];
+    return p;
 }
 
 struct StaticOut {
@@ -1015,6 +1010,9 @@ struct StaticOut {
 };
 
 // The plain build (k_ich_plain) with its scratch carved from the static array.
+// Row codes in tails: -1 the source outgrew the fixed tables; -2 an iteration
+// cap stopped it or it reached a step the reference leaves undefined (the
+// regular build reports both through its per-source flags).
 __global__ void __launch_bounds__(128) k_ich_static(LaneConfig C, StaticOut O) {
     int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     int stride = gridDim.x * blockDim.x;
@@ -1031,6 +1029,10 @@ __global__ void __launch_bounds__(128) k_ich_static(LaneConfig C, StaticOut O) {
             O.tails[r] = -1;  // the source outgrew the static tables
             continue;
         }
+        if (L.flags & (kFlagWatchdog | kFlagUndefined)) {
+            O.tails[r] = -2;
+            continue;
+        }
         for (int j = 0; j < C.M.nv && K > 0; ++j) {
             double d = L.vdist(j);
             if (d == DBL_MAX || j == v) continue;
@@ -1041,7 +1043,8 @@ __global__ void __launch_bounds__(128) k_ich_static(LaneConfig C, StaticOut O) {
             O.dist[row + tail] = d;
             if (++tail == K) break;
         }
-        O.tails[r] = tail;
+        // a back-trace can hit an iteration cap or an undefined step too
+        O.tails[r] = (L.flags & (kFlagWatchdog | kFlagUndefined)) ? -2 : tail;
     }
 }
 
