@@ -105,6 +105,13 @@ typedef struct svg_build_opts {
                                  each run by a whole warp (warp-cooperative heap and table operations), the
                                  rest one per lane; -1 automatic, 0 none */
     int32_t coop_warps;       /* warps that run them (0 automatic) */
+    int32_t vote_wait;        /* batched: most loop iterations a lane waits for the warp's vote to pick its
+                                 kind of step (0 = 8) */
+    int32_t heavy_waves;      /* batched: waves of lanes filled heaviest-first before vertex order (0 = 2) */
+    int32_t heap_factor;      /* batched: first-pass physical window heap = heap_factor x K entries (0 = 3);
+                                 a source that outgrows it is re-run with the full 1023 */
+    int32_t autotune;         /* batched: 1 = use the parameters svg_build_autotune cached on this mesh for
+                                 this K (if any) in place of the fields above and of blocks */
 } svg_build_opts;
 
 typedef struct svg_build_stats {
@@ -136,6 +143,19 @@ void svg_build_opts_default(svg_build_opts* o);
  * build the SVG of mesh m on the device.  The graph stays resident.  Builds
  * from several threads are safe; they run one at a time. */
 svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out);
+
+/* Autotuner (no counterpart in the reference): times full batched builds of
+ * mesh m at opts->K with candidate launch parameters - how many of the
+ * heaviest sources run on whole warps and with how many warps, blocks per SM,
+ * the vote wait limit, the heavy-first waves and the physical heap factor -
+ * one parameter at a time from the current best (at most max_trials builds,
+ * 0 = 16), checks that every candidate builds the same graph (a checksum of
+ * the CSR), and caches the fastest on the mesh for this K: later svg_build
+ * calls with opts.autotune = 1 use it.  *best (optional) receives the chosen
+ * options, *best_ms (optional) its build time.  The parameters change only
+ * the schedule, never the graph. */
+svg_status svg_build_autotune(svg_mesh* m, const svg_build_opts* opts, int32_t max_trials, svg_build_opts* best,
+                              double* best_ms);
 
 svg_status svg_graph_stats(const svg_graph* g, svg_build_stats* st);
 

@@ -55,7 +55,8 @@ class BuildOptions(C.Structure):
         ("threads_per_block", C.c_int32), ("blocks", C.c_int32), ("with_paths", C.c_int32),
         ("heavy_first", C.c_int32), ("hbm_budget", C.c_int64),
         ("source_begin", C.c_int32), ("source_end", C.c_int32),
-        ("coop_sources", C.c_int32), ("coop_warps", C.c_int32),
+        ("coop_sources", C.c_int32), ("coop_warps", C.c_int32), ("vote_wait", C.c_int32),
+        ("heavy_waves", C.c_int32), ("heap_factor", C.c_int32), ("autotune", C.c_int32),
     ]
 
 
@@ -109,7 +110,7 @@ EXPORTS = [
     "svg_server_submit_build", "svg_server_submit_sssd", "svg_server_submit_msad", "svg_server_wait",
     "svg_server_poll", "svg_server_take", "svg_server_stats", "svg_server_submit_msad_into",
     "svg_device_memory", "svg_graph_set_query_form", "svg_server_resident",
-    "svg_msad_batch_paths", "svg_sssd_path", "svg_device_fp64_rate",
+    "svg_msad_batch_paths", "svg_sssd_path", "svg_device_fp64_rate", "svg_build_autotune",
 ]
 
 _lib = None
@@ -135,6 +136,8 @@ def lib() -> C.CDLL:
     L.svg_build_opts_default.argtypes = [C.POINTER(BuildOptions)]
     L.svg_build_opts_default.restype = None
     L.svg_build.argtypes = [_P, C.POINTER(BuildOptions), C.POINTER(_P)]
+    L.svg_build_autotune.argtypes = [_P, C.POINTER(BuildOptions), C.c_int32, C.POINTER(BuildOptions),
+                                     C.POINTER(C.c_double)]
     L.svg_graph_stats.argtypes = [_P, C.POINTER(BuildStats)]
     L.svg_graph_source_stats.argtypes = [_P, _P, _P, _P]
     L.svg_graph_free.argtypes = [_P]
@@ -271,6 +274,22 @@ class SVG:
         _check(lib().svg_build(self.mesh._h, C.byref(o), C.byref(h)))
         self._g = h
         return self.stats()
+
+    def autotune(self, max_trials: int = 16, **kw) -> tuple:
+        """svg_build_autotune: time candidate schedules of the batched build of
+        this mesh at K, cache the fastest on the mesh (later ConstructSVG calls
+        with autotune=1 use it).  Returns (chosen options as a dict, build ms)."""
+        if self.mesh is None:
+            raise SvgError(6, "AssignMesh first")
+        o = BuildOptions()
+        lib().svg_build_opts_default(C.byref(o))
+        o.K, o.split_coef, o.vert_coef = self.K, self.splitInfoCoef, self.vertInfoCoef
+        for k, v in kw.items():
+            setattr(o, k, v)
+        best = BuildOptions()
+        ms = C.c_double()
+        _check(lib().svg_build_autotune(self.mesh._h, C.byref(o), int(max_trials), C.byref(best), C.byref(ms)))
+        return {f: getattr(best, f) for f, _ in BuildOptions._fields_}, ms.value
 
     def FreeSVGStructure(self) -> None:
         if self._g:

@@ -326,14 +326,24 @@ void svg_build_opts_default(svg_build_opts* o) {
     o->coop_sources = -1;
 }
 
+}  // extern "C"
+
+namespace {
+// Builds share the lane-scratch arena and run one at a time (a serving loop's
+// builder thread and a caller's thread may both build).
+std::mutex& build_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+}  // namespace
+
+extern "C" {
+
 svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out) {
     return guarded([&]() -> svg_status {
         if (!m || !opts || !out) throw SvgError{SVG_ERR_ARG, "null argument"};
         *out = nullptr;
-        // builds share the lane-scratch arena and run one at a time (a serving
-        // loop's builder thread and a caller's thread may both build)
-        static std::mutex build_mu;
-        std::lock_guard<std::mutex> lock(build_mu);
+        std::lock_guard<std::mutex> lock(build_mutex());
         svg_graph* g = new svg_graph();
         g->mesh = m;
         try {
@@ -345,6 +355,15 @@ svg_status svg_build(svg_mesh* m, const svg_build_opts* opts, svg_graph** out) {
         }
         *out = g;
         return SVG_OK;
+    });
+}
+
+svg_status svg_build_autotune(svg_mesh* m, const svg_build_opts* opts, int32_t max_trials, svg_build_opts* best,
+                              double* best_ms) {
+    return guarded([&]() -> svg_status {
+        if (!m || !opts) throw SvgError{SVG_ERR_ARG, "null argument"};
+        std::lock_guard<std::mutex> lk(build_mutex());
+        return run_autotune(m, *opts, max_trials, best, best_ms);
     });
 }
 

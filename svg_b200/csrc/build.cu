@@ -55,9 +55,17 @@ struct PhaseOut {
     int32_t* st_maxq;
     int32_t* st_flags;
     unsigned long long* acc;       // windows, generated, pseudo-sources, queue-drop sources
+    // Cooperative warps: the first coop_warps warps of the grid each take the
+    // heaviest sources order[0 .. coop_n) one at a time from their own queue
+    // head (coop_work) and run each with the whole warp; then, like every
+    // other warp, one source per lane from order[coop_n ..).
+    int32_t coop_n;
+    int32_t coop_warps;
+    int32_t* coop_work;
 };
 
-__device__ void record_stats(const Lane& L, const PhaseOut& O, int v) {
+template <class LaneType>
+__device__ void record_stats(const LaneType& L, const PhaseOut& O, int v) {
     O.st_windows[v] = L.windows;
     O.st_maxq[v] = L.maxw;
     int f = 0;
@@ -83,7 +91,8 @@ __device__ void record_stats(const Lane& L, const PhaseOut& O, int v) {
 // direct loads; the whole warp walks each finished lane's list 32 entries at a
 // time (the other lanes would only wait), and a ballot keeps the candidates
 // in list order.  Every lane of the warp calls it.
-__device__ void finish_warp(Lane& L, const PhaseOut& O, int v, unsigned amask) {
+template <class LaneType>
+__device__ void finish_warp(LaneType& L, const PhaseOut& O, int v, unsigned amask) {
     constexpr unsigned kFull = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const DevMesh& M = L.C.M;
@@ -184,18 +193,12 @@ __device__ void finish_warp(Lane& L, const PhaseOut& O, int v, unsigned amask) {
 }
 
 // Longest a lane waits for its action type to be chosen (iterations).
-#ifndef SVG_HEAVY_WAVES
-#define SVG_HEAVY_WAVES 2  // waves of lanes filled heaviest-first before vertex order resumes
-#endif
-#ifndef SVG_ICH_MAX_WAIT
-#define SVG_ICH_MAX_WAIT 8
-#endif
 
 // Persistent batched build.  Each lane runs one source at a time and pulls
 // the next from the device work queue.  Every iteration the warp votes: each
 // lane's next action is a window pop, a pseudo-source pop or "source done"
 // (export + start the next source); the action type held by the most lanes
-// runs, the other lanes wait - at most SVG_ICH_MAX_WAIT iterations, after
+// runs, the other lanes wait - at most C.max_wait iterations, after
 // which the longest-waiting lane's type runs.  A lane's own sequence of
 // actions is unchanged; only when it takes them is, so the rare, long paths
 // (pseudo-source fans, exports) run with many lanes at once instead of one
@@ -203,8 +206,27 @@ __device__ void finish_warp(Lane& L, const PhaseOut& O, int v, unsigned amask) {
 __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
     constexpr unsigned kFull = 0xFFFFFFFFu;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((gtid >> 5) < O.coop_warps) {
+        // Cooperative phase: the whole warp on one heavy source at a time,
+        // in the scratch of the warp's first lane.
+        const int wbase = gtid & ~31;
+        CoopLane W(C, wbase);
+        for (;;) {
+            int rc = 0;
+            if ((threadIdx.x & 31) == 0) rc = atomicAdd(O.coop_work, 1);
+            rc = __shfl_sync(kFull, rc, 0);
+            if (rc >= O.coop_n) break;
+            const int vc = O.order[rc];
+            W.begin(vc, false);
+            while (!W.step()) {
+            }
+            finish_warp(W, O, vc, 1u);  // every thread holds the source's state: lane 0 is its owner
+        }
+        if ((threadIdx.x & 31) == 0) W.save_epoch(wbase);
+        __syncwarp();
+    }
     Lane L(C, gtid);
-    int r = atomicAdd(O.work, 1);
+    int r = O.coop_n + atomicAdd(O.work, 1);
     int v = r < O.nsrc ? O.order[r] : -1;
     if (v >= 0) L.begin(v, false);
     int waited = 0;
@@ -214,7 +236,7 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
         const unsigned m1 = __ballot_sync(kFull, act == Lane::kActPseudo);
         const unsigned m2 = __ballot_sync(kFull, act == Lane::kActDone);
         if ((m0 | m1 | m2) == 0) break;
-        const unsigned starving = __ballot_sync(kFull, act >= 0 && waited >= SVG_ICH_MAX_WAIT);
+        const unsigned starving = __ballot_sync(kFull, act >= 0 && waited >= C.max_wait);
         int chosen;
         if (starving) {
             chosen = __shfl_sync(kFull, act, __ffs(starving) - 1);
@@ -231,7 +253,7 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
             } else if (chosen == Lane::kActPseudo) {
                 L.act_pseudo(amask);
             } else {
-                r = atomicAdd(O.work, 1);
+                r = O.coop_n + atomicAdd(O.work, 1);
                 v = r < O.nsrc ? O.order[r] : -1;
                 if (v >= 0) L.begin(v, false);
             }
@@ -253,10 +275,10 @@ __device__ bool trace_full(Lane& L, int vert, uint32_t& se, double& sx, uint32_t
     int guard = 0;
     for (;;) {
         int s = L.vfind(curVert);
-        double d = s < 0 ? DBL_MAX : L.VT[s].dist;
+        double d = s < 0 ? DBL_MAX : L.VT()[s].dist;
         if (d == 0.0) break;
         if (++guard > M.nf + 8) { L.flags |= kFlagWatchdog; return true; }
-        int enterEdge = s < 0 ? -1 : L.VT[s].enter;
+        int enterEdge = s < 0 ? -1 : L.VT()[s].enter;
         if (enterEdge == -1) {
             if (de == 0xFFFFFFFFu) { de = (uint32_t)__ldg(&M.vr[curVert].first); dx = 0.0; }
             else { se = (uint32_t)__ldg(&M.vr[curVert].first); sx = 0.0; }
@@ -274,8 +296,8 @@ __device__ bool trace_full(Lane& L, int vert, uint32_t& se, double& sx, uint32_t
             continue;
         }
         int ss = L.sfind(enterEdge);
-        double gpos = ss < 0 ? DBL_MAX : L.ST[ss].x;
-        int psrc = ss < 0 ? -1 : L.ST[ss].psrc;
+        double gpos = ss < 0 ? DBL_MAX : L.ST()[ss].x;
+        int psrc = ss < 0 ? -1 : L.ST()[ss].psrc;
         int gid = enterEdge;
         if (de == 0xFFFFFFFFu) { de = (uint32_t)gid; dx = gpos; }
         else { se = (uint32_t)gid; sx = gpos; }
@@ -568,7 +590,31 @@ int ilog2_ceil(int64_t x) {
 
 }  // namespace
 
-svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
+namespace {
+// Options a build runs with: the caller's, or, with autotune set, the
+// launch parameters svg_build_autotune cached on the mesh for this K.
+svg_build_opts effective_options(const svg_mesh* m, const svg_build_opts& o) {
+    svg_build_opts e = o;
+    if (o.autotune && o.mode != SVG_BUILD_PLAIN) {
+        for (const auto& t : m->tuned)
+            if (t.K == o.K) {
+                e.coop_sources = t.opts.coop_sources;
+                e.coop_warps = t.opts.coop_warps;
+                e.vote_wait = t.opts.vote_wait;
+                e.heavy_waves = t.opts.heavy_waves;
+                e.heap_factor = t.opts.heap_factor;
+                e.blocks = t.opts.blocks;
+            }
+    }
+    if (e.vote_wait <= 0) e.vote_wait = 8;
+    if (e.heavy_waves <= 0) e.heavy_waves = 2;
+    if (e.heap_factor <= 0) e.heap_factor = 3;
+    return e;
+}
+}  // namespace
+
+svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
+    const svg_build_opts o = effective_options(m, o_in);
     upload_mesh(m);
     cudaStream_t st = lib_stream();
     const HostMesh& H = m->h;
@@ -622,13 +668,16 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     // windows up to ~2.3K, pseudo-sources up to ~1.3K); a source that needs more is re-run
     // by the retry pass with physical = logical capacity.  The plain build
     // always uses the full capacity.
-    C.wphys = plain ? C.wcap : std::min<int32_t>(C.wcap, std::max<int32_t>(128, (3 * K + 63) / 64 * 64));
+    C.wphys = plain ? C.wcap
+                    : std::min<int32_t>(C.wcap,
+                                        std::max<int32_t>(128, (int32_t)(((int64_t)o.heap_factor * K + 63) / 64 * 64)));
     C.pphys = plain ? C.pcap : std::min<int32_t>(C.pcap, std::max<int32_t>(128, (K + K / 2 + 64 + 63) / 64 * 64));
     C.wstride = heap_stride(C.wphys);
     C.pstride = heap_stride(C.pphys);
     C.vref = (uint32_t)K * o.vert_coef;
     C.sref = (uint32_t)K * o.split_coef;
     C.watchdog = (int64_t)1 << 26;
+    C.max_wait = o.vote_wait;
     Layout lay;
     lay.wphys = C.wphys;
     lay.pphys = C.pphys;
@@ -669,6 +718,7 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
 
     // per-build buffers
     DevBuf b_order, b_misc, b_cand, b_candstart;
+    int32_t coop_n = 0, coop_warps = 0;
     b_order.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1));
     int32_t* d_order = b_order.as<int32_t>();
     bool ordered = false;
@@ -680,7 +730,7 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
         // order 13 % slower on the 72.9K height field).
         std::vector<int32_t> ord((size_t)nsrc);
         for (int32_t i = 0; i < nsrc; ++i) ord[(size_t)i] = sb + i;
-        const int64_t head = std::min<int64_t>(nsrc, (int64_t)lay.lanes * SVG_HEAVY_WAVES);
+        const int64_t head = std::min<int64_t>(nsrc, (int64_t)lay.lanes * o.heavy_waves);
         std::vector<int32_t> byc(ord);
         std::stable_sort(byc.begin(), byc.end(),
                          [&](int32_t a, int32_t b) { return m->cost[(size_t)a] > m->cost[(size_t)b]; });
@@ -692,6 +742,28 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
         int64_t k = head;
         for (int32_t i = 0; i < nsrc; ++i)
             if (!taken[(size_t)i]) ord[(size_t)k++] = sb + i;
+        // The heaviest sources set the build's tail: one lane runs a source's
+        // windows strictly one after another.  The cooperative warps run the
+        // sources whose cost exceeds a lane's average share of the whole build
+        // (the rest of the lanes finish about then), a whole warp each, with
+        // fewer and shorter memory round trips per window.
+        if (o.coop_sources != 0) {
+            double total = 0.0;
+            for (int32_t i = 0; i < nsrc; ++i) total += (double)m->cost[(size_t)(sb + i)];
+            const double share = total / (double)lay.lanes;
+            int64_t n = 0;
+            if (o.coop_sources > 0) {
+                n = std::min<int64_t>(o.coop_sources, nsrc);
+            } else {
+                while (n < head && (double)m->cost[(size_t)ord[(size_t)n]] >= share) ++n;
+                n = std::min<int64_t>(n, lay.lanes / 64);
+            }
+            const int64_t warps = (int64_t)lay.lanes / 32;
+            coop_n = (int32_t)n;
+            coop_warps = (int32_t)std::min<int64_t>(
+                {o.coop_warps > 0 ? (int64_t)o.coop_warps : std::max<int64_t>(1, n / 2), n, warps / 2});
+            if (coop_warps <= 0) coop_n = 0;
+        }
         SVG_CUDA(cudaMemcpyAsync(d_order, ord.data(), sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, st));
         SVG_CUDA(cudaStreamSynchronize(st));
         ordered = true;
@@ -734,6 +806,9 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     O.st_maxq = g->st_maxq;
     O.st_flags = g->st_flags;
     O.acc = d_acc;
+    O.coop_n = coop_n;
+    O.coop_warps = coop_warps;
+    O.coop_work = d_work + 4;
 
     cudaEvent_t ev[4];
     for (auto& e : ev) SVG_CUDA(cudaEventCreate(&e));
@@ -808,6 +883,8 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
                 carve(g_arena[1], l2, C2, st);
                 scratch_bytes += (int64_t)(lane_bytes(l2) * l2.lanes);
                 PhaseOut O2 = O;
+                O2.coop_n = 0;
+                O2.coop_warps = 0;
                 O2.order = d_retry;
                 O2.nsrc = retry_n;
                 O2.work = d_work + 2;  // fresh queue head
@@ -909,6 +986,8 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     S.retried_sources = retry_n;
     S.launches = launches;
     S.scratch_bytes = scratch_bytes;
+    S.coop_sources = coop_n;
+    S.coop_warps = coop_warps;
     (void)t03;
     // flag tallies; per-source costs kept on the mesh for the next build's order
     std::vector<int32_t> fl((size_t)nv);
@@ -928,6 +1007,161 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
         if (f & 4) ++S.watchdog_sources;
         if (f & 8) ++S.undefined_sources;
     }
+    return SVG_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+
+namespace {
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+// Order-independent checksum of a CSR: the sum of a mix of every (row, edge
+// position, neighbour, length bits); equal graphs give equal sums.
+__global__ void k_csr_checksum(const int64_t* off, const int32_t* adj, const double* dist, int32_t nv,
+                               unsigned long long* out) {
+    unsigned long long acc = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = off[v], e = off[v + 1];
+        acc += mix64(((unsigned long long)v << 20) ^ (unsigned long long)(e - b));
+        for (int64_t i = b; i < e; ++i)
+            acc += mix64(((unsigned long long)(uint32_t)adj[i] << 32 | (unsigned long long)(i - b)) ^
+                         mix64((unsigned long long)__double_as_longlong(dist[i])));
+    }
+    atomicAdd(out, acc);
+}
+
+unsigned long long csr_checksum(const svg_graph* g) {
+    cudaStream_t st = lib_stream();
+    unsigned long long* d = dev_alloc_n<unsigned long long>(1);
+    SVG_CUDA(cudaMemsetAsync(d, 0, sizeof(*d), st));
+    k_csr_checksum<<<256, 256, 0, st>>>(g->off, g->adj, g->dist, g->nv, d);
+    SVG_CUDA(cudaGetLastError());
+    unsigned long long h = 0;
+    SVG_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    dev_free(d);
+    return h;
+}
+}  // namespace
+
+// Coordinate descent over the batched build's schedule parameters, each
+// candidate timed as a full build (device time, CUDA events): the
+// cooperative share (how many of the heaviest sources run on whole warps,
+// then with how many warps), blocks per SM, the vote wait limit, the
+// heavy-first waves and the physical heap factor.  A candidate replaces the
+// best only when at least 2 % faster (one timing each).  Every candidate
+// must build the graph of the first (checksum), else the tuner fails.
+svg_status run_autotune(svg_mesh* m, const svg_build_opts& in, int32_t max_trials, svg_build_opts* out,
+                        double* out_ms) {
+    if (in.mode == SVG_BUILD_PLAIN) throw SvgError{SVG_ERR_ARG, "the autotuner tunes the batched build"};
+    if (max_trials <= 0) max_trials = 16;
+    svg_build_opts base = in;
+    base.autotune = 0;
+    if (base.heavy_first == 0) base.heavy_first = 1;
+    base.coop_sources = -1;
+    base.coop_warps = 0;
+    base.vote_wait = 8;
+    base.heavy_waves = 2;
+    base.heap_factor = 3;
+    base.blocks = 0;
+    int trials = 0;
+    unsigned long long ref_sum = 0;
+    bool have_ref = false;
+    svg_build_stats last{};
+    auto trial = [&](const svg_build_opts& o) -> double {
+        svg_graph g;
+        g.mesh = m;
+        try {
+            run_build(m, o, &g);
+            const unsigned long long h = csr_checksum(&g);
+            if (have_ref && h != ref_sum) throw SvgError{SVG_ERR_STATE, "autotune: a candidate built a different graph"};
+            ref_sum = h;
+            have_ref = true;
+        } catch (...) {
+            free_graph_device(&g);
+            throw;
+        }
+        last = g.stats;
+        free_graph_device(&g);
+        ++trials;
+        return last.ms_total;
+    };
+    trial(base);                   // records the per-source costs at this K (the work order)
+    double best_ms = trial(base);  // the defaults, timed with that order
+    svg_build_opts best = base;
+    const int32_t n_auto = last.coop_sources;
+    auto consider = [&](const svg_build_opts& o) {
+        if (trials >= max_trials) return;
+        const double ms = trial(o);
+        if (ms < 0.98 * best_ms) {
+            best_ms = ms;
+            best = o;
+        }
+    };
+    // threads per source: how many of the heaviest sources run on whole warps
+    for (int32_t n : {0, n_auto / 2, n_auto * 2, n_auto * 4}) {
+        if (n == n_auto || (n == 0 && n_auto == 0) || (n > 0 && n == n_auto / 2 && n_auto < 2)) continue;
+        svg_build_opts o = best;
+        o.coop_sources = n;
+        o.coop_warps = std::max(1, n / 2);
+        consider(o);
+    }
+    if (best.coop_sources != 0) {
+        const int32_t n = best.coop_sources > 0 ? best.coop_sources : n_auto;
+        if (n > 0)
+            for (int32_t w : {std::max(1, n / 4), n}) {
+                svg_build_opts o = best;
+                o.coop_sources = n;
+                o.coop_warps = w;
+                consider(o);
+            }
+    }
+    // occupancy: one block of lanes per SM fewer than fit
+    {
+        int per_sm = 0, dev = 0, sms = 0;
+        SVG_CUDA(cudaGetDevice(&dev));
+        SVG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        SVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ich_batched, 128, 0));
+        if (per_sm > 1) {
+            svg_build_opts o = best;
+            o.blocks = (per_sm - 1) * sms;
+            consider(o);
+        }
+    }
+    for (int32_t w : {4, 16}) {
+        svg_build_opts o = best;
+        o.vote_wait = w;
+        consider(o);
+    }
+    for (int32_t w : {1, 4}) {
+        svg_build_opts o = best;
+        o.heavy_waves = w;
+        consider(o);
+    }
+    for (int32_t f : {2, 4}) {
+        svg_build_opts o = best;
+        o.heap_factor = f;
+        consider(o);
+    }
+    bool found = false;
+    for (auto& t : m->tuned)
+        if (t.K == in.K) {
+            t.opts = best;
+            t.ms = best_ms;
+            found = true;
+        }
+    if (!found) m->tuned.push_back({in.K, best, best_ms});
+    if (out) {
+        *out = best;
+        out->autotune = 1;
+    }
+    if (out_ms) *out_ms = best_ms;
     return SVG_OK;
 }
 

@@ -75,6 +75,13 @@ struct svg_mesh {
     // heaviest first (longest-processing-time first).
     int32_t cost_K = 0;
     std::vector<int32_t> cost;
+    // Launch parameters svg_build_autotune chose, per K.
+    struct Tuned {
+        int32_t K;
+        svg_build_opts opts;
+        double ms;
+    };
+    std::vector<Tuned> tuned;
 };
 
 struct svg_qctx;
@@ -115,6 +122,8 @@ struct svg_qctx {
 
 namespace svgb {
 svg_status run_build(svg_mesh* m, const svg_build_opts& o, svg_graph* g);
+svg_status run_autotune(svg_mesh* m, const svg_build_opts& o, int32_t max_trials, svg_build_opts* best,
+                        double* best_ms);
 void upload_mesh(svg_mesh* m);
 void free_graph_device(svg_graph* g);
 svg_status run_sssd(svg_graph* g, int32_t n, const int32_t* d_s, const int32_t* d_t, double* d_dist);

@@ -19,6 +19,19 @@
 //   vertex table: 32-byte slots, open addressing, epoch-stamped (no clears);
 //   split table : 32-byte slots, same scheme;
 //   vertex list : table slots in insertion order (the emission walks only these).
+//
+// Two forms of a lane, the same algorithm and arithmetic:
+//   LaneT<false>  one thread runs one source (the batched kernel's lanes, the
+//                 plain and allocation-free builds);
+//   LaneT<true>   a whole warp runs one heavy source: every thread holds the
+//                 same state and runs the same scalar code (stores of one
+//                 value by all threads are one store), while the memory-bound
+//                 parts use the 32 threads - a sift-up loads every ancestor in
+//                 one round trip and decides by ballot, a sift-down loads the
+//                 five levels below a node in one round trip, and table
+//                 lookups probe 8 slots of up to 4 keys at once.  The heap and
+//                 table contents and the order of every operation are those
+//                 of the one-thread form, so the results are bit-identical.
 #pragma once
 
 #include <cfloat>
@@ -104,6 +117,7 @@ struct LaneConfig {
     int32_t vcap_log2, scap_log2;
     int32_t vlimit, slimit;  // max keys this lane's tables take before kFlagCapacity
     int64_t watchdog;        // max steps per source
+    int32_t max_wait;        // batched kernel: most iterations a lane waits for the vote to pick its step
     WinEntry* wheap;
     WinPay* wpool;
     uint16_t* wfree;
@@ -174,15 +188,113 @@ __device__ __forceinline__ void finish_window(double b0, double b1, double d0, d
     w.p.psd = psd;
 }
 
-struct Lane {
+// Group probe of up to four keys in 32-byte open-addressing slots (key at
+// byte 0, epoch at byte 4): threads 8g..8g+7 walk key g's chain 8 slots per
+// round, a ballot finds the first empty slot and any match before it (linear
+// probing stops at the first empty slot, as the one-thread probes do).  Every
+// thread of the warp calls it with the same arguments and receives the same
+// results: slot (-1 if absent), the slot's two 16-byte halves, and the first
+// empty slot of the chain (where an insert goes).
+struct ProbeQ {
+    const char* tbl;
+    uint32_t mask;
+    uint32_t h0;
+    uint32_t key;
+    bool on;
+};
+struct ProbeR {
+    int slot;
+    int empty;
+    int4 head;
+    int4 tail;
+};
+__device__ __forceinline__ void coop_probe4(const ProbeQ& q0, const ProbeQ& q1, const ProbeQ& q2, const ProbeQ& q3,
+                                            uint32_t epoch, ProbeR& r0, ProbeR& r1, ProbeR& r2, ProbeR& r3) {
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, grp = lane >> 3, gl = lane & 7;
+    // this thread's query, by value (a reference chosen by a thread-dependent
+    // index would put the four queries in local memory)
+    const char* q_tbl = grp == 0 ? q0.tbl : grp == 1 ? q1.tbl : grp == 2 ? q2.tbl : q3.tbl;
+    const uint32_t q_mask = grp == 0 ? q0.mask : grp == 1 ? q1.mask : grp == 2 ? q2.mask : q3.mask;
+    const uint32_t q_h0 = grp == 0 ? q0.h0 : grp == 1 ? q1.h0 : grp == 2 ? q2.h0 : q3.h0;
+    const uint32_t q_key = grp == 0 ? q0.key : grp == 1 ? q1.key : grp == 2 ? q2.key : q3.key;
+    r0.slot = r1.slot = r2.slot = r3.slot = -1;
+    r0.empty = r1.empty = r2.empty = r3.empty = -1;
+    unsigned open = (q0.on ? 0x000000FFu : 0u) | (q1.on ? 0x0000FF00u : 0u) | (q2.on ? 0x00FF0000u : 0u) |
+                    (q3.on ? 0xFF000000u : 0u);
+    for (uint32_t base = 0; open; base += 8) {
+        const bool mine = (open >> lane) & 1u;
+        const uint32_t h = (q_h0 + base + (uint32_t)gl) & q_mask;
+        int4 hd = make_int4(0, 0, 0, 0), tl = hd;
+        if (mine) {
+            const int4* sp = reinterpret_cast<const int4*>(q_tbl + (size_t)h * 32);
+            hd = sp[0];
+            tl = sp[1];
+        }
+        const bool empty = mine && (uint32_t)hd.y != epoch;
+        const bool hit = mine && !empty && (uint32_t)hd.x == q_key;
+        const unsigned me = __ballot_sync(kFull, empty), mh = __ballot_sync(kFull, hit);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            ProbeR& r = g == 0 ? r0 : g == 1 ? r1 : g == 2 ? r2 : r3;
+            const ProbeQ& qg = g == 0 ? q0 : g == 1 ? q1 : g == 2 ? q2 : q3;
+            if (!((open >> (8 * g)) & 1u)) continue;
+            const unsigned ge = (me >> (8 * g)) & 0xFFu, gh = (mh >> (8 * g)) & 0xFFu;
+            const int fe = ge ? __ffs(ge) - 1 : 8;
+            const unsigned hb = fe < 8 ? (gh & ((1u << fe) - 1u)) : gh;
+            if (hb) {
+                const int src = 8 * g + __ffs(hb) - 1;
+                r.slot = (int)((qg.h0 + base + (uint32_t)(src - 8 * g)) & qg.mask);
+                r.head.x = __shfl_sync(kFull, hd.x, src);
+                r.head.y = __shfl_sync(kFull, hd.y, src);
+                r.head.z = __shfl_sync(kFull, hd.z, src);
+                r.head.w = __shfl_sync(kFull, hd.w, src);
+                r.tail.x = __shfl_sync(kFull, tl.x, src);
+                r.tail.y = __shfl_sync(kFull, tl.y, src);
+                r.tail.z = __shfl_sync(kFull, tl.z, src);
+                r.tail.w = __shfl_sync(kFull, tl.w, src);
+                open &= ~(0xFFu << (8 * g));
+            } else if (fe < 8) {
+                r.empty = (int)((qg.h0 + base + (uint32_t)fe) & qg.mask);
+                open &= ~(0xFFu << (8 * g));
+            } else if (base > qg.mask) {  // a full table with no empty slot: absent, nowhere to insert
+                open &= ~(0xFFu << (8 * g));
+            }
+        }
+    }
+}
+__device__ __forceinline__ ProbeQ probe_q(const void* tbl, int log2cap, uint32_t key, bool on) {
+    ProbeQ q;
+    q.tbl = static_cast<const char*>(tbl);
+    q.mask = (1u << log2cap) - 1u;
+    q.h0 = (key * 0x9E3779B1u) >> (32 - log2cap);
+    q.key = key;
+    q.on = on;
+    return q;
+}
+__device__ __forceinline__ ProbeQ probe_off() {
+    ProbeQ q;
+    q.tbl = nullptr;
+    q.mask = 0;
+    q.h0 = 0;
+    q.key = 0;
+    q.on = false;
+    return q;
+}
+
+template <bool kCoop>
+struct LaneT {
     const LaneConfig& C;
-    WinEntry* WH;   // this lane's heap column (stride 32 entries)
-    PsEntry* PH;
-    WinPay* WP;
-    uint16_t* WF;
-    VSlot* VT;
-    int32_t* VL;
-    SSlot* ST;
+    // This lane's scratch, derived from its index when used (held pointers
+    // would take fourteen registers for the whole loop).
+    int32_t lid;
+    __device__ __forceinline__ WinEntry* WH() const { return C.wheap + (size_t)lid * C.wstride; }
+    __device__ __forceinline__ PsEntry* PH() const { return C.pheap + (size_t)lid * C.pstride; }
+    __device__ __forceinline__ WinPay* WP() const { return C.wpool + (size_t)lid * C.wphys; }
+    __device__ __forceinline__ uint16_t* WF() const { return C.wfree + (size_t)lid * C.wphys; }
+    __device__ __forceinline__ VSlot* VT() const { return C.vtab + ((size_t)lid << C.vcap_log2); }
+    __device__ __forceinline__ int32_t* VL() const { return C.vlist + (size_t)lid * C.vlimit; }
+    __device__ __forceinline__ SSlot* ST() const { return C.stab + ((size_t)lid << C.scap_log2); }
     int wsize, psize, nfree, nfresh;
     int vcount, scount;
     uint32_t epoch;
@@ -193,29 +305,33 @@ struct Lane {
     int windows, pseudos, generated, maxw, maxp;
     int64_t steps;
 
-    __device__ Lane(const LaneConfig& c, int gtid) : C(c) {
-        WH = C.wheap + (size_t)gtid * C.wstride;
-        PH = C.pheap + (size_t)gtid * C.pstride;
-        WP = C.wpool + (size_t)gtid * C.wphys;
-        WF = C.wfree + (size_t)gtid * C.wphys;
-        VT = C.vtab + ((size_t)gtid << C.vcap_log2);
-        VL = C.vlist + (size_t)gtid * C.vlimit;
-        ST = C.stab + ((size_t)gtid << C.scap_log2);
+    // gtid: the thread's global index (one-thread form) or the warp's first
+    // thread's (cooperative form: the warp uses that thread's scratch).
+    __device__ LaneT(const LaneConfig& c, int gtid) : C(c) {
+        lid = gtid;
         epoch = C.epochs[gtid];
     }
 
-    __device__ __forceinline__ WinEntry& wh(int i) { return WH[i]; }
-    __device__ __forceinline__ PsEntry& ph(int i) { return PH[i]; }
+    __device__ __forceinline__ WinEntry& wh(int i) { return WH()[i]; }
+    __device__ __forceinline__ PsEntry& ph(int i) { return PH()[i]; }
 
     // ---------------------------------------------------------- tables
     __device__ __forceinline__ uint32_t vhash(uint32_t k) const { return (k * 0x9E3779B1u) >> (32 - C.vcap_log2); }
     __device__ __forceinline__ uint32_t shash(uint32_t k) const { return (k * 0x9E3779B1u) >> (32 - C.scap_log2); }
 
+    // One key's group probe (cooperative form).
+    __device__ __forceinline__ ProbeR probe1(const void* tbl, int log2cap, uint32_t key) const {
+        ProbeR r0, r1, r2, r3;
+        coop_probe4(probe_q(tbl, log2cap, key, true), probe_off(), probe_off(), probe_off(), epoch, r0, r1, r2, r3);
+        return r0;
+    }
+
     // slot index of vertex v, or -1 if absent
     __device__ __forceinline__ int vfind(int v) {
+        if constexpr (kCoop) return probe1(VT(), C.vcap_log2, (uint32_t)v).slot;
         uint32_t mask = (1u << C.vcap_log2) - 1, h = vhash((uint32_t)v);
         for (;;) {
-            uint2 ke = *reinterpret_cast<const uint2*>(&VT[h]);
+            uint2 ke = *reinterpret_cast<const uint2*>(&VT()[h]);
             if (ke.y != epoch) return -1;
             if (ke.x == (uint32_t)v) return (int)h;
             h = (h + 1) & mask;
@@ -225,8 +341,8 @@ struct Lane {
     // and the distance (one 32-byte sector).  vfinish completes the probe chain.
     __device__ __forceinline__ void vfirst(int v, uint32_t& h, int4& k, double& d) const {
         h = vhash((uint32_t)v);
-        k = *reinterpret_cast<const int4*>(&VT[h]);
-        d = VT[h].dist;
+        k = *reinterpret_cast<const int4*>(&VT()[h]);
+        d = VT()[h].dist;
     }
     __device__ __forceinline__ int vfinish(int v, uint32_t h, int4& k, double& d) const {
         const uint32_t mask = (1u << C.vcap_log2) - 1;
@@ -234,14 +350,14 @@ struct Lane {
             if ((uint32_t)k.y != epoch) { d = DBL_MAX; return -1; }
             if ((uint32_t)k.x == (uint32_t)v) return (int)h;
             h = (h + 1) & mask;
-            k = *reinterpret_cast<const int4*>(&VT[h]);
-            d = VT[h].dist;
+            k = *reinterpret_cast<const int4*>(&VT()[h]);
+            d = VT()[h].dist;
         }
     }
     __device__ __forceinline__ void sfirst(int e, uint32_t& h, int4& k, double2& dx) const {
         h = shash((uint32_t)e);
-        k = *reinterpret_cast<const int4*>(&ST[h]);
-        dx = *reinterpret_cast<const double2*>(&ST[h].dist);
+        k = *reinterpret_cast<const int4*>(&ST()[h]);
+        dx = *reinterpret_cast<const double2*>(&ST()[h].dist);
     }
     // returns the slot or -1; dx = {dist, x} of the entry, {DBL_MAX, DBL_MAX} if absent
     __device__ __forceinline__ int sfinish(int e, uint32_t h, int4& k, double2& dx) const {
@@ -250,26 +366,34 @@ struct Lane {
             if ((uint32_t)k.y != epoch) { dx.x = DBL_MAX; dx.y = DBL_MAX; return -1; }
             if ((uint32_t)k.x == (uint32_t)e) return (int)h;
             h = (h + 1) & mask;
-            k = *reinterpret_cast<const int4*>(&ST[h]);
-            dx = *reinterpret_cast<const double2*>(&ST[h].dist);
+            k = *reinterpret_cast<const int4*>(&ST()[h]);
+            dx = *reinterpret_cast<const double2*>(&ST()[h].dist);
         }
     }
     __device__ __forceinline__ double vdist(int v) {
         int s = vfind(v);
-        return s < 0 ? DBL_MAX : VT[s].dist;
+        return s < 0 ? DBL_MAX : VT()[s].dist;
     }
     __device__ __forceinline__ int vbirth(int v) {
         int s = vfind(v);
-        return s < 0 ? -1 : VT[s].birth;
+        return s < 0 ? -1 : VT()[s].birth;
     }
     // MyHashTable::operator[] (MyHashTable.cuh:72-82): find or insert with defaults
     __device__ int vput(int v) {
-        uint32_t mask = (1u << C.vcap_log2) - 1, h = vhash((uint32_t)v);
-        for (;;) {
-            uint2 ke = *reinterpret_cast<const uint2*>(&VT[h]);
-            if (ke.y != epoch) break;
-            if (ke.x == (uint32_t)v) return (int)h;
-            h = (h + 1) & mask;
+        uint32_t h;
+        if constexpr (kCoop) {
+            const ProbeR r = probe1(VT(), C.vcap_log2, (uint32_t)v);
+            if (r.slot >= 0) return r.slot;
+            h = (uint32_t)r.empty;  // vlimit keeps a quarter of the slots empty: never -1
+        } else {
+            uint32_t mask = (1u << C.vcap_log2) - 1;
+            h = vhash((uint32_t)v);
+            for (;;) {
+                uint2 ke = *reinterpret_cast<const uint2*>(&VT()[h]);
+                if (ke.y != epoch) break;
+                if (ke.x == (uint32_t)v) return (int)h;
+                h = (h + 1) & mask;
+            }
         }
         if (vcount >= C.vlimit) {  // keep the probe chains short: hand the source to the big pass
             flags |= kFlagCapacity;
@@ -277,28 +401,37 @@ struct Lane {
         }
         VSlot s;
         s.key = (uint32_t)v; s.epoch = epoch; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.sslot = -1; s.pad = 0;
-        VT[h] = s;
-        VL[vcount] = (int32_t)h;
+        VT()[h] = s;
+        VL()[vcount] = (int32_t)h;
         ++vcount;
         if ((uint32_t)vcount > C.vref) flags |= kFlagRefOverflow;
         return (int)h;
     }
     __device__ __forceinline__ int sfind(int e) {
+        if constexpr (kCoop) return probe1(ST(), C.scap_log2, (uint32_t)e).slot;
         uint32_t mask = (1u << C.scap_log2) - 1, h = shash((uint32_t)e);
         for (;;) {
-            uint2 ke = *reinterpret_cast<const uint2*>(&ST[h]);
+            uint2 ke = *reinterpret_cast<const uint2*>(&ST()[h]);
             if (ke.y != epoch) return -1;
             if (ke.x == (uint32_t)e) return (int)h;
             h = (h + 1) & mask;
         }
     }
     __device__ int sput(int e) {
-        uint32_t mask = (1u << C.scap_log2) - 1, h = shash((uint32_t)e);
-        for (;;) {
-            uint2 ke = *reinterpret_cast<const uint2*>(&ST[h]);
-            if (ke.y != epoch) break;
-            if (ke.x == (uint32_t)e) return (int)h;
-            h = (h + 1) & mask;
+        uint32_t h;
+        if constexpr (kCoop) {
+            const ProbeR r = probe1(ST(), C.scap_log2, (uint32_t)e);
+            if (r.slot >= 0) return r.slot;
+            h = (uint32_t)r.empty;  // slimit keeps a quarter of the slots empty: never -1
+        } else {
+            uint32_t mask = (1u << C.scap_log2) - 1;
+            h = shash((uint32_t)e);
+            for (;;) {
+                uint2 ke = *reinterpret_cast<const uint2*>(&ST()[h]);
+                if (ke.y != epoch) break;
+                if (ke.x == (uint32_t)e) return (int)h;
+                h = (h + 1) & mask;
+            }
         }
         if (scount >= C.slimit) {
             flags |= kFlagCapacity;
@@ -306,7 +439,7 @@ struct Lane {
         }
         SSlot s;
         s.key = (uint32_t)e; s.epoch = epoch; s.psrc = -1; s.pad = 0; s.dist = DBL_MAX; s.x = DBL_MAX;
-        ST[h] = s;
+        ST()[h] = s;
         ++scount;
         if ((uint32_t)scount > C.sref) flags |= kFlagRefOverflow;
         return (int)h;
@@ -316,12 +449,12 @@ struct Lane {
         for (int i = 0; i < (1 << C.vcap_log2); ++i) {
             VSlot s;
             s.key = 0xFFFFFFFFu; s.epoch = 0; s.enter = -1; s.birth = -1; s.dist = DBL_MAX; s.sslot = -1; s.pad = 0;
-            VT[i] = s;
+            VT()[i] = s;
         }
         for (int i = 0; i < (1 << C.scap_log2); ++i) {
             SSlot s;
             s.key = 0xFFFFFFFFu; s.epoch = 0; s.psrc = -1; s.pad = 0; s.dist = DBL_MAX; s.x = DBL_MAX;
-            ST[i] = s;
+            ST()[i] = s;
         }
     }
 
@@ -337,17 +470,38 @@ struct Lane {
     // by level.
     template <class T>
     __device__ __forceinline__ void sift_up(T* H, int cur, const T& x) {
-        T anc[4];
+        if constexpr (kCoop) {
+            // thread j holds ancestor cur >> (j + 1); the moves are the
+            // ancestors, from the parent up, whose key exceeds x's
+            const int lane = threadIdx.x & 31;
+            const int a = lane < 30 ? (cur >> (lane + 1)) : 0;
+            T e;
+            e.key = 0.0;
+            if (a > 0) e = H[a];
+            const unsigned gt = __ballot_sync(0xFFFFFFFFu, a > 0 && e.key > x.key);
+            const int m = __ffs(~gt) - 1;
+            if (lane < m) H[cur >> lane] = e;
+            H[cur >> m] = x;
+            __syncwarp();
+            return;
+        }
+        // keys of the first four ancestors in one round trip; the moved
+        // entries are read again (their sectors were just fetched) before
+        // each is written one level down
+        double ak[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if ((cur >> (j + 1)) > 0) anc[j] = H[cur >> (j + 1)];
+        for (int j = 0; j < 4; ++j) ak[j] = (cur >> (j + 1)) > 0 ? H[cur >> (j + 1)].key : 0.0;
         int m = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            if (m == j && (cur >> (j + 1)) > 0 && anc[j].key > x.key) m = j + 1;
+            if (m == j && (cur >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
+        T mv[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            if (j < m) H[cur >> j] = anc[j];
+            if (j < m) mv[j] = H[cur >> (j + 1)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < m) H[cur >> j] = mv[j];
         int c = cur >> m;
         if (m == 4) {
             for (;;) {
@@ -373,55 +527,104 @@ struct Lane {
             flags |= kFlagCapacity;
             return;
         }
-        const int slot = nfree > 0 ? (int)WF[--nfree] : nfresh++;
-        WP[slot] = w.p;
+        const int slot = nfree > 0 ? (int)WF()[--nfree] : nfresh++;
+        WP()[slot] = w.p;
         WinEntry e;
         e.key = w.key;
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        sift_up(WH, ++wsize, e);
+        sift_up(WH(), ++wsize, e);
         if (wsize > maxw) maxw = wsize;
     }
+    // Cooperative sift-down: the 62 nodes 1-5 levels below `cur` are loaded
+    // in one round trip (two per thread: node k, k+32 of the subtree in level
+    // order), the path is chosen level by level from shuffled keys with the
+    // rules below, and each moved node is written by the thread holding it.
+    // Every node is read before any write of that round, and a round writes
+    // only nodes above the next round's subtree.
+    template <class T>
+    __device__ __forceinline__ int coop_sift_down(T* H, int n, const T& last) {
+        constexpr unsigned kFull = 0xFFFFFFFFu;
+        const int lane = threadIdx.x & 31;
+        int cur = 1;
+        for (int round = 0; round < 8; ++round) {
+            if ((cur << 1) > n) break;
+            T e[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int k = lane + 32 * r;       // subtree node in level order
+                const int d = 31 - __clz(k + 2);   // its depth below cur (1..5)
+                const int ix = k < 62 ? (cur << d) + (k + 2 - (1 << d)) : n + 1;
+                e[r].key = 0.0;
+                if (ix <= n) e[r] = H[ix];
+            }
+            int p = cur;
+            bool moved_all = true;
+#pragma unroll
+            for (int d = 1; d <= 5; ++d) {
+                const int l = p << 1;
+                if (l > n) { moved_all = false; break; }
+                const int kl = l - (cur << d) + (1 << d) - 2;  // subtree position of l (l + 1 is kl + 1)
+                const double al = __shfl_sync(kFull, (kl >> 5) ? e[1].key : e[0].key, kl & 31);
+                const double bl = __shfl_sync(kFull, ((kl + 1) >> 5) ? e[1].key : e[0].key, (kl + 1) & 31);
+                const int k1 = (l + 1 <= n && !(al < bl)) ? 1 : 0;
+                if (!((k1 ? bl : al) < last.key)) { moved_all = false; break; }
+                const int kc = kl + k1;
+                if (lane == (kc & 31)) H[p] = (kc >> 5) ? e[1] : e[0];
+                p = l + k1;
+            }
+            cur = p;
+            if (!moved_all) break;
+        }
+        __syncwarp();
+        return cur;
+    }
+
     // The reference's sift-down (PriorityQueue.cuh:76-105): the children of
     // `cur` are compared with each other (ties go right) and the smaller moves
-    // up while it is smaller than the last element.  The children and
-    // grandchildren of `cur` are loaded together, so two levels cost one
+    // up while it is smaller than the last element.  The keys of the children
+    // and grandchildren of `cur` are loaded together, so two levels cost one
     // dependent round trip (reads past the heap's end stay inside the lane's
-    // array, stride >= cap + 4, and are never used); the two levels are written
-    // with selects and predicated stores, one exit test per two levels.
+    // array, stride >= cap + 4, and are never used); the moved entries are read
+    // again from the sectors just fetched and written with predicated stores,
+    // one exit test per two levels.
     template <class T>
     __device__ __forceinline__ int sift_down2(T* H, int n, const T& last) {
+        if constexpr (kCoop) return coop_sift_down(H, n, last);
         int cur = 1;
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
-            const T a = H[l], b = H[l + 1];
+            const double a = H[l].key, b = H[l + 1].key;
             const int g = cur << 2;
-            T q0, q1, q2, q3;
-            if (g <= n) { q0 = H[g]; q1 = H[g + 1]; q2 = H[g + 2]; q3 = H[g + 3]; }
-            const int k1 = (l + 1 <= n && !(a.key < b.key)) ? 1 : 0;
-            const T e1 = k1 ? b : a;
-            const bool mv1 = e1.key < last.key;
+            double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+            if (g <= n) { q0 = H[g].key; q1 = H[g + 1].key; q2 = H[g + 2].key; q3 = H[g + 3].key; }
+            const int k1 = (l + 1 <= n && !(a < b)) ? 1 : 0;
+            const bool mv1 = (k1 ? b : a) < last.key;
             const int c1 = l + k1;
             const int l2 = c1 << 1;
-            const T a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
-            const int k2 = (l2 + 1 <= n && !(a2.key < b2.key)) ? 1 : 0;
-            const T e2 = k2 ? b2 : a2;
-            const bool mv2 = mv1 && l2 <= n && e2.key < last.key;
+            const double a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
+            const int k2 = (l2 + 1 <= n && !(a2 < b2)) ? 1 : 0;
+            const bool mv2 = mv1 && l2 <= n && (k2 ? b2 : a2) < last.key;
+            const int c2 = l2 + k2;
+            T e1, e2;
+            if (mv1) e1 = H[c1];
+            if (mv2) e2 = H[c2];
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
-            cur = mv2 ? l2 + k2 : (mv1 ? c1 : cur);
+            cur = mv2 ? c2 : (mv1 ? c1 : cur);
             if (!mv2) break;
         }
         return cur;
     }
     __device__ WinEntry wpop() {
-        WinEntry top = WH[1];
-        WinEntry last = WH[wsize];
+        WinEntry top = WH()[1];
+        WinEntry last = WH()[wsize];
         const int n = --wsize;
-        const int cur = sift_down2(WH, n, last);
-        WH[cur] = last;
-        WF[nfree++] = (uint16_t)(top.sb & 0xFFFF);
+        const int cur = sift_down2(WH(), n, last);
+        WH()[cur] = last;
+        WF()[nfree++] = (uint16_t)(top.sb & 0xFFFF);
+        if constexpr (kCoop) __syncwarp();
         return top;
     }
     __device__ void ppush(double key, int vert, int level, int birth) {
@@ -433,25 +636,30 @@ struct Lane {
             flags |= kFlagCapacity;
             return;
         }
-        int cur = ++psize, p = cur >> 1;
-        while (p > 0) {
-            PsEntry pe = ph(p);
-            if (!(pe.key > key)) break;
-            ph(cur) = pe;
-            cur = p;
-            p = cur >> 1;
-        }
         PsEntry e;
         e.key = key; e.vert = vert; e.lb = ((uint32_t)level << 8) | (uint32_t)(birth & 0xFF);
-        ph(cur) = e;
+        if constexpr (kCoop) {
+            sift_up(PH(), ++psize, e);
+        } else {
+            int cur = ++psize, p = cur >> 1;
+            while (p > 0) {
+                PsEntry pe = ph(p);
+                if (!(pe.key > key)) break;
+                ph(cur) = pe;
+                cur = p;
+                p = cur >> 1;
+            }
+            ph(cur) = e;
+        }
         if (psize > maxp) maxp = psize;
     }
     __device__ PsEntry ppop() {
-        PsEntry top = PH[1];
-        PsEntry last = PH[psize];
+        PsEntry top = PH()[1];
+        PsEntry last = PH()[psize];
         const int n = --psize;
-        const int cur = sift_down2(PH, n, last);
-        PH[cur] = last;
+        const int cur = sift_down2(PH(), n, last);
+        PH()[cur] = last;
+        if constexpr (kCoop) __syncwarp();
         return top;
     }
 
@@ -480,7 +688,7 @@ struct Lane {
 
     // write the birth of vertex slot s, keeping the source's cached birth
     __device__ __forceinline__ void set_birth(int s, int v, int b) {
-        VT[s].birth = b;
+        VT()[s].birth = b;
         if (v == source) src_birth = b;
     }
 
@@ -508,30 +716,30 @@ struct Lane {
             int opv = hc.v1;
             int s = vput(opv);
             if (s < 0) return;
-            if (hc.len > VT[s].dist) {
+            if (hc.len > VT()[s].dist) {
                 cur = hc.twin;
                 if (cur != -1) cur = nxt(cur);
                 continue;
             }
             set_birth(s, opv, 0);
-            VT[s].dist = hc.len;
-            VT[s].enter = hc.twin;
-            VT[s].sslot = -1;
+            VT()[s].dist = hc.len;
+            VT()[s].enter = hc.twin;
+            VT()[s].sslot = -1;
             if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE)) {
                 cur = hc.twin;
                 if (cur != -1) cur = nxt(cur);
                 continue;
             }
-            ppush(hc.len, opv, 0, VT[s].birth);
+            ppush(hc.len, opv, 0, VT()[s].birth);
             cur = hc.twin;
             if (cur != -1) cur = nxt(cur);
         } while (cur != start && cur != -1);
         int s = vput(source);
         if (s < 0) return;
         set_birth(s, source, 0);
-        VT[s].dist = 0.0;
-        VT[s].enter = -1;
-        VT[s].sslot = -1;
+        VT()[s].dist = 0.0;
+        VT()[s].enter = -1;
+        VT()[s].sslot = -1;
     }
 
     // ICHDevice::IsValidWindow (ICHDevice.cu:906-955) given the distances d1,
@@ -602,14 +810,31 @@ struct Lane {
             A = h0.v0;
             B = h0.v1;
             Cv = h1.v1;
-            vfirst(A, hA, kA, dA);
-            vfirst(B, hB, kB, dB);
-            vfirst(Cv, hC, kC, dC);
-            sfirst(e0, hS, kS, sdx);
-            vfinish(A, hA, kA, dA);
-            vfinish(B, hB, kB, dB);
-            sC = vfinish(Cv, hC, kC, dC);
-            sS = sfinish(e0, hS, kS, sdx);
+            if constexpr (!kCoop) {
+                vfirst(A, hA, kA, dA);
+                vfirst(B, hB, kB, dB);
+                vfirst(Cv, hC, kC, dC);
+                sfirst(e0, hS, kS, sdx);
+                vfinish(A, hA, kA, dA);
+                vfinish(B, hB, kB, dB);
+                sC = vfinish(Cv, hC, kC, dC);
+                sS = sfinish(e0, hS, kS, sdx);
+            }
+        }
+        if constexpr (kCoop) {  // the four lookups in one group probe (live is the same in every thread)
+            ProbeR ra, rb, rc, rs;
+            coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)A, live), probe_q(VT(), C.vcap_log2, (uint32_t)B, live),
+                        probe_q(VT(), C.vcap_log2, (uint32_t)Cv, live), probe_q(ST(), C.scap_log2, (uint32_t)e0, live),
+                        epoch, ra, rb, rc, rs);
+            dA = ra.slot >= 0 ? __hiloint2double(ra.tail.y, ra.tail.x) : DBL_MAX;
+            dB = rb.slot >= 0 ? __hiloint2double(rb.tail.y, rb.tail.x) : DBL_MAX;
+            dC = rc.slot >= 0 ? __hiloint2double(rc.tail.y, rc.tail.x) : DBL_MAX;
+            sC = rc.slot;
+            kC = rc.head;
+            sS = rs.slot;
+            sdx = rs.slot >= 0 ? make_double2(__hiloint2double(rs.tail.y, rs.tail.x),
+                                              __hiloint2double(rs.tail.w, rs.tail.z))
+                               : make_double2(DBL_MAX, DBL_MAX);
         }
         __syncwarp(amask);
 
@@ -638,9 +863,9 @@ struct Lane {
                         if (ssl < 0) {
                             ok = false;  // table full: the source goes to the retry pass
                         } else {
-                            ST[ssl].dist = D;
-                            ST[ssl].psrc = psrc;
-                            ST[ssl].x = l0 - interX;
+                            ST()[ssl].dist = D;
+                            ST()[ssl].psrc = psrc;
+                            ST()[ssl].x = l0 - interX;
                         }
                     }
                     if (ok && D < dC) {
@@ -651,9 +876,9 @@ struct Lane {
                         } else {
                             const int b = (int)(signed char)((sC >= 0 ? kC.w : -1) + 1);
                             set_birth(s, Cv, b);
-                            VT[s].dist = D;
-                            VT[s].enter = e0;
-                            VT[s].sslot = ssl;  // D < dC <= split distance: the entry was just written
+                            VT()[s].dist = D;
+                            VT()[s].enter = e0;
+                            VT()[s].sslot = ssl;  // D < dC <= split distance: the entry was just written
                             dC = D;  // the children's tests read the updated distance
                             if (__ldg(&M.vr[Cv].flags) & kVertSaddleGT) ppush(D, Cv, win.level + 1, b);
                         }
@@ -716,8 +941,8 @@ struct Lane {
         int startEdge = -1, endEdge = -1;
         if (live) {
             int vs = vfind(pv);
-            int enter = vs < 0 ? -1 : VT[vs].enter;
-            int vb = vs < 0 ? -1 : VT[vs].birth;
+            int enter = vs < 0 ? -1 : VT()[vs].enter;
+            int vb = vs < 0 ? -1 : VT()[vs].birth;
             if (enter == -1 && vb != -1) {
                 startEdge = __ldg(&M.vr[pv].first);
                 endEdge = startEdge;
@@ -729,7 +954,7 @@ struct Lane {
                 HeRec h0 = ld_he(M.he, e0), h1 = ld_he(M.he, e1), h2 = ld_he(M.he, e2);
                 double l0 = h0.len, l1 = h1.len, l2 = h2.len;
                 int ss = sfind(e0);
-                double sx = ss < 0 ? DBL_MAX : ST[ss].x;
+                double sx = ss < 0 ? DBL_MAX : ST()[ss].x;
                 double ex = l0 - sx, ey = 0.0;
                 double2 v2 = ld_apex(M.geo, e0);
                 double dx = ex - v2.x, dy = ey - v2.y;
@@ -776,7 +1001,7 @@ struct Lane {
                 HeRec hc = ld_he(M.he, cur);
                 int opv = hc.v1;
                 int os = vfind(opv);
-                double od = os < 0 ? DBL_MAX : VT[os].dist;
+                double od = os < 0 ? DBL_MAX : VT()[os].dist;
                 if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE) || od < pdist + hc.len) {
                     cur = hc.twin;
                     if (cur != -1) cur = nxt(cur);
@@ -785,12 +1010,12 @@ struct Lane {
                 if (od == DBL_MAX) ++total;
                 int s = os < 0 ? vput(opv) : os;
                 if (s < 0) break;
-                VT[s].dist = pdist + hc.len;
-                int b = (int)(signed char)(VT[s].birth + 1);
+                VT()[s].dist = pdist + hc.len;
+                int b = (int)(signed char)(VT()[s].birth + 1);
                 set_birth(s, opv, b);
-                VT[s].enter = hc.twin;
-                VT[s].sslot = -1;
-                ppush(VT[s].dist, opv, plevel, b);
+                VT()[s].enter = hc.twin;
+                VT()[s].sslot = -1;
+                ppush(VT()[s].dist, opv, plevel, b);
                 cur = hc.twin;
                 if (cur != -1) cur = nxt(cur);
             } while (cur != start && cur != -1);
@@ -849,19 +1074,28 @@ struct Lane {
         }
         pk_w.key = 0.0; pk_w.psrc = 0; pk_w.sb = 0;
         pk_p.key = 0.0; pk_p.vert = 0; pk_p.lb = 0;
-        if (wsize > 0) pk_w = WH[1];
-        if (psize > 0) pk_p = PH[1];
+        if (wsize > 0) pk_w = WH()[1];
+        if (psize > 0) pk_p = PH()[1];
         // both birth lookups issued together
         const bool wlook = wsize > 0 && pk_w.psrc != source;
         const bool plook = psize > 0;
-        uint32_t hw = 0, hp = 0;
-        int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
-        double dw = 0.0, dp = 0.0;
-        if (wlook) vfirst(pk_w.psrc, hw, kw, dw);
-        if (plook) vfirst(pk_p.vert, hp, kp, dp);
         int wb = src_birth, pb = -1;
-        if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
-        if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+        if constexpr (kCoop) {
+            ProbeR rw, rp, r2, r3;
+            coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pk_w.psrc, wlook),
+                        probe_q(VT(), C.vcap_log2, (uint32_t)pk_p.vert, plook), probe_off(), probe_off(), epoch, rw,
+                        rp, r2, r3);
+            if (wlook) wb = rw.slot < 0 ? -1 : rw.head.w;
+            if (plook) pb = rp.slot < 0 ? -1 : rp.head.w;
+        } else {
+            uint32_t hw = 0, hp = 0;
+            int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
+            double dw = 0.0, dp = 0.0;
+            if (wlook) vfirst(pk_w.psrc, hw, kw, dw);
+            if (plook) vfirst(pk_p.vert, hp, kp, dp);
+            if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
+            if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+        }
         const bool wstale = wsize > 0 && (int)(signed char)(pk_w.sb >> 16) != wb;
         if (wstale) return pk_act = kActWindow;
         const bool pstale = psize > 0 && (int)(signed char)(pk_p.lb & 0xFF) != pb;
@@ -883,7 +1117,7 @@ struct Lane {
         WinPay pay;
         pay.cross = -1;
         pay.level = 0;
-        if (proc) pay = WP[t.sb & 0xFFFF];  // issued before the sift-down
+        if (proc) pay = WP()[t.sb & 0xFFFF];  // issued before the sift-down
         wpop();
         __syncwarp(amask);
         const bool live = proc && !(pay.level > C.M.nf);
@@ -905,9 +1139,10 @@ struct Lane {
         if (live && C.K != -1 && total >= C.K) done = true;
     }
 
-    // peek + act for one lane on its own; true when finished.
+    // peek + act for one lane on its own (or, cooperative, for the whole
+    // warp on its source); true when finished.
     __device__ bool step() {
-        const unsigned self = 1u << (threadIdx.x & 31);
+        const unsigned self = kCoop ? 0xFFFFFFFFu : 1u << (threadIdx.x & 31);
         const int a = peek<0>();
         if (a == kActDone) return true;
         if (a == kActWindow) act_window(self);
@@ -915,6 +1150,8 @@ struct Lane {
         return false;
     }
 };
+using Lane = LaneT<false>;
+using CoopLane = LaneT<true>;
 
 // ICHDevice::BuildGeodesicPathTo(vertex) (ICHDevice.cu:336-480) for a
 // vertex whose path reaches the source through windows only: walk back from

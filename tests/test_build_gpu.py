@@ -51,6 +51,86 @@ def test_build_matches_reference_golden(name, K, mode):
     assert st["watchdog_sources"] == 0
 
 
+def coop_build(pos, faces, K, coop_warps=8, coop_sources=None, **kw):
+    """Batched build whose work order comes from a first build's per-source
+    costs, with the heaviest `coop_sources` (default: every source) run by
+    whole warps (the cooperative form)."""
+    m = Mesh.from_arrays(pos, faces)
+    s = SVG()
+    s.AssignMesh(m)
+    s.SetParameters(K, kw.pop("split_coef", 10), kw.pop("vert_coef", 2))
+    s.ConstructSVG(heavy_first=0, **kw)   # records the per-source costs on the mesh
+    n = len(pos) if coop_sources is None else coop_sources
+    st = s.ConstructSVG(heavy_first=1, coop_sources=n, coop_warps=coop_warps, **kw)
+    off, nodes = s.CopySVGToHost()
+    return off, nodes, st, s, m
+
+
+@pytest.mark.parametrize("name,K", golden_params())
+def test_cooperative_form_matches_reference_golden(name, K):
+    """Every source run by a whole warp: the same rows as the reference."""
+    g = load_golden(name)
+    off, nodes, st, s, _ = coop_build(g["pos"], g["faces"], K)
+    assert st["coop_sources"] == len(g["pos"])
+    _, _, flags = s.source_stats()
+    goff, gnodes = rows_from_padded(g[f"K{K}_tails"], g[f"K{K}_nodes"])
+    ok_rows = [r for r in range(len(off) - 1) if not (flags[r] & 2)]
+    assert compare_rows(off, nodes, goff, gnodes, rows=ok_rows) == []
+    if st["ref_overflow_sources"] == 0:
+        assert st["windows_generated"] == int(g[f"K{K}_stats"][:, 0].sum())
+
+
+@pytest.mark.parametrize("cfg,K,n", [(1, 500, 1200), (0, 100, 1500)])
+def test_cooperative_form_matches_oracle_on_benchmark_mesh_samples(cfg, K, n):
+    """The heaviest sources of a leading source range run cooperatively (with
+    the 1023-entry queue cap binding at K=500), the rest one per lane."""
+    pos, faces = meshgen.config_mesh(cfg)
+    off, nodes, st, _, _ = coop_build(pos, faces, K, coop_warps=32, coop_sources=n // 3,
+                                      source_begin=0, source_end=n)
+    assert st["coop_sources"] == n // 3
+    (ooff, onodes), rows = _oracle_rows(pos, faces, K, np.arange(0, n, dtype=np.int32))
+    assert compare_rows(off[:n + 1], nodes[:off[n]], ooff, onodes) == []
+    assert st["windows_generated"] == int(rows.stats[:, 0].sum())
+
+
+def test_automatic_cooperative_share_keeps_the_graph():
+    """The automatic choice (heaviest sources above a lane's average share)
+    gives the same CSR as a build with no cooperative warps."""
+    pos, faces = meshgen.config_mesh(1, 0.3)
+    outs, counts = [], []
+    for coop in (0, -1):
+        m = Mesh.from_arrays(pos, faces)
+        g = SVG()
+        g.AssignMesh(m)
+        g.SetParameters(300)
+        g.ConstructSVG(heavy_first=0)
+        st = g.ConstructSVG(heavy_first=1, coop_sources=coop)
+        counts.append(st["coop_sources"])
+        outs.append(g.csr())
+    assert counts[0] == 0
+    for x, y in zip(outs[0], outs[1]):
+        assert np.array_equal(x, y)
+
+
+def test_autotuned_schedule_keeps_the_graph():
+    """The tuner's candidates and its choice change the schedule only: the
+    tuned build equals a default build bit for bit (the tuner itself also
+    checks every candidate's CSR checksum against the first)."""
+    pos, faces = meshgen.config_mesh(1, 0.25)
+    m = Mesh.from_arrays(pos, faces)
+    g = SVG()
+    g.AssignMesh(m)
+    g.SetParameters(200)
+    g.ConstructSVG(heavy_first=0)
+    ref = g.csr()
+    best, ms = g.autotune(max_trials=12)
+    assert best["autotune"] == 1 and ms > 0
+    g.ConstructSVG(autotune=1)
+    got = g.csr()
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)
+
+
 def test_reference_table_overflow_is_flagged():
     """monkey, K=6: the centre reaches 13 vertices, the reference's vertex
     table holds 2K = 12 keys."""
