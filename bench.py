@@ -1062,6 +1062,7 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=400)
     ap.add_argument("--plain-seconds", type=float, default=30.0)
     ap.add_argument("--record", default="", help="also write the JSON line to this file")
+    ap.add_argument("--no-autotune", action="store_true", help="time the default schedule, not the tuned one")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: N whole builds (weak scaling) instead of one build sharded by source range")
     args = ap.parse_args()
@@ -1134,9 +1135,9 @@ def main():
         a = C.c_double()
         L.svg_timer_mark(C.byref(a))
         if sharded:
-            st = svg.ConstructSVG(mode=mode, source_begin=sb, source_end=se)
+            st = svg.ConstructSVG(mode=mode, source_begin=sb, source_end=se, autotune=int(tune))
         else:
-            st = svg.ConstructSVG(mode=mode)
+            st = svg.ConstructSVG(mode=mode, autotune=int(tune))
         b = C.c_double()
         L.svg_timer_mark(C.byref(b))
         ms = b.value
@@ -1144,6 +1145,17 @@ def main():
             ms += gather_slices()
         return ms, st
 
+    # untimed: the autotuner times candidate schedules of this build (the
+    # graph is the same for all of them) and caches the fastest on the mesh
+    tune = not args.no_autotune
+    tuned = None
+    if tune:
+        t0 = time.perf_counter()
+        kw = dict(source_begin=sb, source_end=se) if shard else {}
+        best, best_ms = svg.autotune(max_trials=16, **kw)
+        tuned = {"params": {k: best[k] for k in ("coop_sources", "coop_warps", "blocks", "vote_wait",
+                                                 "heavy_waves", "heap_factor")},
+                 "tuned_build_ms": best_ms, "tuning_s": time.perf_counter() - t0}
     for _ in range(args.warmup):
         timed_build()
     barrier(dist)
@@ -1233,9 +1245,10 @@ def main():
                            parallelism=(f"shard{ws}: contiguous source ranges, CSR slices all-gathered over NCCL"
                                         if shard else f"replicas{ws}"),
                            edges_per_build=edges_per_build, windows_per_build=windows_per_build,
-                           work_order="timed steps: heaviest sources first for two waves (per-source costs "
-                                      "recorded by the warm-up builds), then vertex order; e2e: a fresh mesh "
-                                      "every step, ordered by a K/10 probe build inside the timed region"),
+                           work_order="timed steps: the autotuned schedule (untimed tuning before the warm-up; "
+                                      "heaviest sources first, the heaviest on whole warps, by the per-source "
+                                      "costs the earlier builds recorded); e2e: a fresh mesh every step with the "
+                                      "default schedule, ordered by a K/10 probe build inside the timed region"),
             "build_s": total_ms_max / args.steps / 1e3,
             "kernel_ms_per_step": statistics.mean(kern),
             "roofline": roofline_figures(st, peaks, fma_rate()),
@@ -1244,6 +1257,8 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_max / args.steps},
             "gpu_launches": launches,
+            "autotune": tuned,
+            "coop": {"sources": st["coop_sources"], "warps": st["coop_warps"]},
             "clocks": ck,
             "flags": {k: st[k] for k in ("queue_drop_sources", "ref_overflow_sources", "watchdog_sources",
                                          "undefined_sources", "retried_sources")},
