@@ -42,6 +42,10 @@
 #ifndef SVG_ICH_INLINE_STALE
 #define SVG_ICH_INLINE_STALE 8
 #endif
+// 1: peek() prefetches into L1 the face records the next window step reads
+#ifndef SVG_FACE_PREFETCH
+#define SVG_FACE_PREFETCH 1
+#endif
 
 namespace svgb {
 
@@ -1061,6 +1065,22 @@ struct LaneT {
         }
     }
 
+    // L1 prefetch of the records propagate() reads for a window crossing
+    // half-edge e0: the three half-edges of its face and their unfolded
+    // geometry (one 32-byte sector each).  The window is popped and propagated
+    // after the warp's vote and the sift-down; by then these are in L1
+    // instead of a DRAM round trip away.  A prefetch has no result and no
+    // fault, so a window that turns out stale costs six sector reads.
+    __device__ __forceinline__ void prefetch_face(int e0) const {
+        const int e1 = nxt(e0), e2 = nxt(e1);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e0));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e1));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e2));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e0));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e1));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e2));
+    }
+
     __device__ int peek_once() {
         pk_proc = false;
         if (done || (wsize == 0 && psize == 0) || (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined))) {
@@ -1093,8 +1113,13 @@ struct LaneT {
             double dw = 0.0, dp = 0.0;
             if (wlook) vfirst(pk_w.psrc, hw, kw, dw);
             if (plook) vfirst(pk_p.vert, hp, kp, dp);
+            // the top window's half-edge, loaded in the same round trip as the
+            // birth probes (its sector is the payload's, read again when the
+            // window is popped)
+            const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
             if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
             if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+            if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
         }
         const bool wstale = wsize > 0 && (int)(signed char)(pk_w.sb >> 16) != wb;
         if (wstale) return pk_act = kActWindow;
