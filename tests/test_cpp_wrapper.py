@@ -94,7 +94,7 @@ def test_cpp_driver_matches_python_path():
                 f.write(f"{s} {t}\n")
             f.write(f"{pairs[0][0]} {pairs[0][0]}\n")  # s == t
             for st, w in zip(sets, wts):
-                f.write("m %d %s\n" % (len(st), " ".join(f"{a} {b!r}" for a, b in zip(st, w))))
+                f.write("m %d %s\n" % (len(st), " ".join(f"{int(a)} {float(b)!r}" for a, b in zip(st, w))))
         r = subprocess.run([exe, obj, str(K), qf], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr
         cpp_file = open(os.path.join(td, "torus.svg"), "rb").read()
