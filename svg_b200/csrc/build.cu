@@ -55,10 +55,11 @@ struct PhaseOut {
     int32_t* st_maxq;
     int32_t* st_flags;
     unsigned long long* acc;       // windows, generated, pseudo-sources, queue-drop sources
-    // Cooperative warps: the first coop_warps warps of the grid each take the
-    // heaviest sources order[0 .. coop_n) one at a time from their own queue
-    // head (coop_work) and run each with the whole warp; then, like every
-    // other warp, one source per lane from order[coop_n ..).
+    // Cooperative warps: warp 0 of each of the first coop_warps blocks takes
+    // the heaviest sources order[0 .. coop_n) one at a time from its own
+    // queue head (coop_work) and runs each with the whole warp, its two heaps
+    // in the block's shared memory; then, like every other warp, it runs one
+    // source per lane from order[coop_n ..).
     int32_t coop_n;
     int32_t coop_warps;
     int32_t* coop_work;
@@ -206,11 +207,14 @@ __device__ void finish_warp(LaneType& L, const PhaseOut& O, int v, unsigned amas
 __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
     constexpr unsigned kFull = 0xFFFFFFFFu;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((gtid >> 5) < O.coop_warps) {
+    if (threadIdx.x < 32 && (int)blockIdx.x < O.coop_warps) {
         // Cooperative phase: the whole warp on one heavy source at a time,
-        // in the scratch of the warp's first lane.
+        // its heaps in shared memory, its pool and tables in the scratch of
+        // the warp's first lane.
+        extern __shared__ __align__(16) unsigned char s_heaps[];
         const int wbase = gtid & ~31;
         CoopLane W(C, wbase);
+        W.sheap = reinterpret_cast<WinEntry*>(s_heaps);
         for (;;) {
             int rc = 0;
             if ((threadIdx.x & 31) == 0) rc = atomicAdd(O.coop_work, 1);
@@ -760,8 +764,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
             }
             const int64_t warps = (int64_t)lay.lanes / 32;
             coop_n = (int32_t)n;
+            // one cooperative warp per block at most (warp 0, whose block holds its heaps)
             coop_warps = (int32_t)std::min<int64_t>(
-                {o.coop_warps > 0 ? (int64_t)o.coop_warps : std::max<int64_t>(1, n / 2), n, warps / 2});
+                {o.coop_warps > 0 ? (int64_t)o.coop_warps : std::max<int64_t>(1, n / 2), n, warps / 2,
+                 (int64_t)lay.lanes / tpb});
             if (coop_warps <= 0) coop_n = 0;
         }
         SVG_CUDA(cudaMemcpyAsync(d_order, ord.data(), sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, st));
@@ -849,7 +855,13 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
             O.cand = b_cand.as<Cand>();
             O.cand_cap = cap;
             O.cand_start = b_candstart.as<int64_t>();
-            k_ich_batched<<<blocks, tpb, 0, st>>>(C, O);
+            // the cooperative warps' heaps: window then pseudo-source entries
+            const size_t coop_smem =
+                coop_warps > 0 ? ((size_t)C.wstride * sizeof(WinEntry) + (size_t)C.pstride * sizeof(PsEntry)) : 0;
+            if (coop_smem > 48 * 1024)
+                SVG_CUDA(cudaFuncSetAttribute(k_ich_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)coop_smem));
+            k_ich_batched<<<blocks, tpb, coop_smem, st>>>(C, O);
             ++launches;
             SVG_CUDA(cudaGetLastError());
             SVG_CUDA(cudaMemcpyAsync(&retry_n, d_retry_n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));

@@ -292,8 +292,17 @@ struct LaneT {
     // This lane's scratch, derived from its index when used (held pointers
     // would take fourteen registers for the whole loop).
     int32_t lid;
-    __device__ __forceinline__ WinEntry* WH() const { return C.wheap + (size_t)lid * C.wstride; }
-    __device__ __forceinline__ PsEntry* PH() const { return C.pheap + (size_t)lid * C.pstride; }
+    // The cooperative form keeps its source's two heaps in shared memory
+    // (sheap: wstride window entries, then pstride pseudo-source entries).
+    WinEntry* sheap = nullptr;
+    __device__ __forceinline__ WinEntry* WH() const {
+        if constexpr (kCoop) return sheap;
+        return C.wheap + (size_t)lid * C.wstride;
+    }
+    __device__ __forceinline__ PsEntry* PH() const {
+        if constexpr (kCoop) return reinterpret_cast<PsEntry*>(sheap + C.wstride);
+        return C.pheap + (size_t)lid * C.pstride;
+    }
     __device__ __forceinline__ WinPay* WP() const { return C.wpool + (size_t)lid * C.wphys; }
     __device__ __forceinline__ uint16_t* WF() const { return C.wfree + (size_t)lid * C.wphys; }
     __device__ __forceinline__ VSlot* VT() const { return C.vtab + ((size_t)lid << C.vcap_log2); }
