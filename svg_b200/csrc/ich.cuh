@@ -1110,12 +1110,15 @@ struct LaneT {
         const bool plook = psize > 0;
         int wb = src_birth, pb = -1;
         if constexpr (kCoop) {
+            // the top window's half-edge, loaded before the probe's round trip
+            const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
             ProbeR rw, rp, r2, r3;
             coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pk_w.psrc, wlook),
                         probe_q(VT(), C.vcap_log2, (uint32_t)pk_p.vert, plook), probe_off(), probe_off(), epoch, rw,
                         rp, r2, r3);
             if (wlook) wb = rw.slot < 0 ? -1 : rw.head.w;
             if (plook) pb = rp.slot < 0 ? -1 : rp.head.w;
+            if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
         } else {
             uint32_t hw = 0, hp = 0;
             int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
