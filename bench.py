@@ -1193,6 +1193,7 @@ def main():
     out_bufs = (pinned(len(pos) + 1, torch.int64), pinned(nnz0 + 1024, torch.int32),
                 pinned(nnz0 + 1024, torch.float64))
     e2e_ms, e2e_edges, h2d, d2h = [], 0, 0, 0
+    parts = {"mesh_build_upload": [], "build_call": [], "build_device": [], "csr_to_host": []}
     for i in range(args.warmup + args.steps):
         flush_l2()
         a = C.c_double()
@@ -1200,15 +1201,22 @@ def main():
         t0 = time.perf_counter()
         m2 = Mesh.from_arrays(posc, facc)
         m2.copyToGPU()
+        t1 = time.perf_counter()
         s2 = SVG()
         s2.AssignMesh(m2)
         s2.SetParameters(K_BUILD, 10, 2)
         st2 = s2.ConstructSVG(source_begin=sb, source_end=se) if shard else s2.ConstructSVG()
+        t2 = time.perf_counter()
         off, adj, dist_h = s2.csr(out=out_bufs)
         b = C.c_double()
         L.svg_timer_mark(C.byref(b))
-        wall = (time.perf_counter() - t0) * 1e3
+        t3 = time.perf_counter()
+        wall = (t3 - t0) * 1e3
         if i >= args.warmup:
+            parts["mesh_build_upload"].append((t1 - t0) * 1e3)
+            parts["build_call"].append((t2 - t1) * 1e3)
+            parts["build_device"].append(st2["ms_total"])
+            parts["csr_to_host"].append((t3 - t2) * 1e3)
             e2e_ms.append(max(b.value, wall))
             e2e_edges += st2["edges"]
             h2d = m2.edgeNum * 64 + m2.vertNum * (8 + 24)
@@ -1255,7 +1263,9 @@ def main():
             "cpu_baseline": cpu,
             "plain": plain,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_max / args.steps},
+                    "ms_per_step": e2e_max / args.steps,
+                    "breakdown_ms_mean": {k: round(statistics.mean(v), 2) for k, v in parts.items() if v},
+                    "note": "build_call includes the K/10 probe build that orders a fresh mesh's sources"},
             "gpu_launches": launches,
             "autotune": tuned,
             "coop": {"sources": st["coop_sources"], "warps": st["coop_warps"]},
