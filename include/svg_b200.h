@@ -112,6 +112,8 @@ typedef struct svg_build_opts {
                                  a source that outgrows it is re-run with the full 1023 */
     int32_t autotune;         /* batched: 1 = use the parameters svg_build_autotune cached on this mesh for
                                  this K (if any) in place of the fields above and of blocks */
+    int32_t coop_tail;        /* batched: 1 (default) = once the work queue is drained, a warp left with one
+                                 running lane finishes that lane's source on all 32 threads; 0 = off */
 } svg_build_opts;
 
 typedef struct svg_build_stats {

@@ -57,6 +57,7 @@ class BuildOptions(C.Structure):
         ("source_begin", C.c_int32), ("source_end", C.c_int32),
         ("coop_sources", C.c_int32), ("coop_warps", C.c_int32), ("vote_wait", C.c_int32),
         ("heavy_waves", C.c_int32), ("heap_factor", C.c_int32), ("autotune", C.c_int32),
+        ("coop_tail", C.c_int32),
     ]
 
 

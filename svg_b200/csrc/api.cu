@@ -324,6 +324,7 @@ void svg_build_opts_default(svg_build_opts* o) {
     o->with_paths = 1;
     o->heavy_first = 1;
     o->coop_sources = -1;
+    o->coop_tail = 1;
 }
 
 }  // extern "C"

@@ -63,6 +63,9 @@ struct PhaseOut {
     int32_t coop_n;
     int32_t coop_warps;
     int32_t* coop_work;
+    // 1: once the work queue is drained, a warp left with one running lane
+    // finishes that lane's source in the cooperative form
+    int32_t coop_tail;
 };
 
 template <class LaneType>
@@ -234,6 +237,7 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
     int v = r < O.nsrc ? O.order[r] : -1;
     if (v >= 0) L.begin(v, false);
     int waited = 0;
+    int adopt = -1;
     for (;;) {
         const int act = v >= 0 ? L.template peek<SVG_ICH_INLINE_STALE>() : -1;
         const unsigned m0 = __ballot_sync(kFull, act == Lane::kActWindow);
@@ -247,6 +251,12 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
         } else {
             const int c0 = __popc(m0), c1 = __popc(m1), c2 = __popc(m2);
             chosen = (c0 >= c1 && c0 >= c2) ? Lane::kActWindow : (c1 >= c2 ? Lane::kActPseudo : Lane::kActDone);
+        }
+        if (O.coop_tail && m2 == 0 && __popc(m0 | m1) == 1 && __ballot_sync(kFull, v < 0) == ~(m0 | m1)) {
+            // The queue is drained (every other lane found it empty) and one
+            // lane still runs a source: the whole warp adopts it below.
+            adopt = __ffs(m0 | m1) - 1;
+            break;
         }
         const unsigned amask = chosen == Lane::kActWindow ? m0 : (chosen == Lane::kActPseudo ? m1 : m2);
         if (chosen == Lane::kActDone) finish_warp(L, O, v, amask);  // the whole warp exports
@@ -265,7 +275,14 @@ __global__ void SVG_ICH_BOUNDS k_ich_batched(LaneConfig C, PhaseOut O) {
             ++waited;
         }
     }
-    L.save_epoch(gtid);
+    L.save_epoch(gtid);  // adoption below keeps lane `adopt`'s epoch: no begin() runs there
+    if (adopt >= 0) {
+        CoopLane W(C, blockIdx.x * blockDim.x + (threadIdx.x & ~31));
+        W.adopt(L, adopt);
+        while (!W.step()) {
+        }
+        finish_warp(W, O, __shfl_sync(kFull, v, adopt), 1u << adopt);  // lane `adopt`'s scratch; it owns it
+    }
 }
 
 // BuildGeodesicPathTo(vertex) (ICHDevice.cu:336-480), the full back-trace the
@@ -815,6 +832,7 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     O.coop_n = coop_n;
     O.coop_warps = coop_warps;
     O.coop_work = d_work + 4;
+    O.coop_tail = o.coop_tail != 0 ? 1 : 0;
 
     cudaEvent_t ev[4];
     for (auto& e : ev) SVG_CUDA(cudaEventCreate(&e));

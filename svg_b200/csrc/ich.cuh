@@ -293,14 +293,17 @@ struct LaneT {
     // would take fourteen registers for the whole loop).
     int32_t lid;
     // The cooperative form keeps its source's two heaps in shared memory
-    // (sheap: wstride window entries, then pstride pseudo-source entries).
+    // (sheap: wstride window entries, then pstride pseudo-source entries), or,
+    // for a source it adopted from a lane (sheap null), in that lane's scratch.
     WinEntry* sheap = nullptr;
     __device__ __forceinline__ WinEntry* WH() const {
-        if constexpr (kCoop) return sheap;
+        if constexpr (kCoop)
+            if (sheap) return sheap;
         return C.wheap + (size_t)lid * C.wstride;
     }
     __device__ __forceinline__ PsEntry* PH() const {
-        if constexpr (kCoop) return reinterpret_cast<PsEntry*>(sheap + C.wstride);
+        if constexpr (kCoop)
+            if (sheap) return reinterpret_cast<PsEntry*>(sheap + C.wstride);
         return C.pheap + (size_t)lid * C.pstride;
     }
     __device__ __forceinline__ WinPay* WP() const { return C.wpool + (size_t)lid * C.wphys; }
@@ -323,6 +326,37 @@ struct LaneT {
     __device__ LaneT(const LaneConfig& c, int gtid) : C(c) {
         lid = gtid;
         epoch = C.epochs[gtid];
+    }
+
+    // Cooperative form: take over the source lane o of this warp is running
+    // in the one-thread form (every thread calls it; the state comes from
+    // lane o by shuffles, the scratch and heaps stay lane o's).  The adopted
+    // source continues exactly where the lane stood: the next step re-reads
+    // the heap tops the lane's cached look was taken from.
+    template <class Other>
+    __device__ void adopt(const Other& L, int o) {
+        constexpr unsigned kFull = 0xFFFFFFFFu;
+        sheap = nullptr;
+        lid = __shfl_sync(kFull, L.lid, o);
+        wsize = __shfl_sync(kFull, L.wsize, o);
+        psize = __shfl_sync(kFull, L.psize, o);
+        nfree = __shfl_sync(kFull, L.nfree, o);
+        nfresh = __shfl_sync(kFull, L.nfresh, o);
+        vcount = __shfl_sync(kFull, L.vcount, o);
+        scount = __shfl_sync(kFull, L.scount, o);
+        epoch = __shfl_sync(kFull, L.epoch, o);
+        source = __shfl_sync(kFull, L.source, o);
+        src_birth = __shfl_sync(kFull, L.src_birth, o);
+        total = __shfl_sync(kFull, L.total, o);
+        flags = __shfl_sync(kFull, L.flags, o);
+        windows = __shfl_sync(kFull, L.windows, o);
+        pseudos = __shfl_sync(kFull, L.pseudos, o);
+        generated = __shfl_sync(kFull, L.generated, o);
+        maxw = __shfl_sync(kFull, L.maxw, o);
+        maxp = __shfl_sync(kFull, L.maxp, o);
+        steps = __shfl_sync(kFull, L.steps, o);
+        done = __shfl_sync(kFull, (int)L.done, o) != 0;
+        pk_valid = false;
     }
 
     __device__ __forceinline__ WinEntry& wh(int i) { return WH()[i]; }
