@@ -112,6 +112,28 @@ def test_automatic_cooperative_share_keeps_the_graph():
         assert np.array_equal(x, y)
 
 
+def test_tail_adoption_keeps_the_graph():
+    """Warps that adopt their last running lane's source once the queue is
+    drained (the default) build the same CSR as warps that do not, and as
+    the oracle on a sample of rows."""
+    pos, faces = meshgen.config_mesh(1, 0.3)
+    outs = []
+    for tail in (0, 1):
+        m = Mesh.from_arrays(pos, faces)
+        g = SVG()
+        g.AssignMesh(m)
+        g.SetParameters(300)
+        g.ConstructSVG(coop_tail=tail, heavy_first=0)
+        outs.append(g.CopySVGToHost())
+    assert compare_rows(outs[0][0], outs[0][1], outs[1][0], outs[1][1]) == []
+    src = np.arange(0, len(pos), 37, dtype=np.int32)
+    (ooff, onodes), _ = _oracle_rows(pos, faces, 300, src)
+    off, nodes = outs[1]
+    got_off = np.concatenate([[0], np.cumsum(np.diff(off)[src])])
+    got = np.concatenate([nodes[off[v]:off[v + 1]] for v in src])
+    assert compare_rows(got_off, got, ooff, onodes) == []
+
+
 def test_autotuned_schedule_keeps_the_graph():
     """The tuner's candidates and its choice change the schedule only: the
     tuned build equals a default build bit for bit (the tuner itself also
