@@ -668,7 +668,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
             throw;
         }
         free_graph_device(&pg);
-        if ((int32_t)m->cost.size() == nv) m->cost_K = K;  // the probe's costs stand in for K's
+        if ((int32_t)m->cost.size() == nv) {
+            m->cost_K = K;  // the probe's costs stand in for K's
+            m->cost_probe = true;
+        }
     }
 
     int dev = 0;
@@ -768,7 +771,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
         // sources whose cost exceeds a lane's average share of the whole build
         // (the rest of the lanes finish about then), a whole warp each, with
         // fewer and shorter memory round trips per window.
-        if (o.coop_sources != 0) {
+        // The automatic share needs the costs of a build at this K: a K/10 probe
+        // ranks the heaviest sources poorly (on the 72.9K height field its top
+        // 200 hold 27 of K=500's top 200), and the tail adoption covers them.
+        if (o.coop_sources > 0 || (o.coop_sources < 0 && !m->cost_probe)) {
             double total = 0.0;
             for (int32_t i = 0; i < nsrc; ++i) total += (double)m->cost[(size_t)(sb + i)];
             const double share = total / (double)lay.lanes;
@@ -1028,8 +1034,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
         if (m->cost_K != K || (int32_t)m->cost.size() != nv) {
             m->cost.assign((size_t)nv, 0);
             m->cost_K = K;
+            m->cost_probe = false;
         }
         for (int32_t v = sb; v < se; ++v) m->cost[(size_t)v] = w[(size_t)v];
+        if (sb == 0 && se == nv) m->cost_probe = false;
     }
     for (int32_t f : fl) {
         if (f & 1) ++S.queue_drop_sources;

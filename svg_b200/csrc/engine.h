@@ -75,6 +75,8 @@ struct svg_mesh {
     // heaviest first (longest-processing-time first).
     int32_t cost_K = 0;
     std::vector<int32_t> cost;
+    // the costs are a K/10 probe build's stand-in, not a build at cost_K
+    bool cost_probe = false;
     // Launch parameters svg_build_autotune chose, per K.
     struct Tuned {
         int32_t K;
