@@ -1256,7 +1256,8 @@ def main():
                            work_order="timed steps: the autotuned schedule (untimed tuning before the warm-up; "
                                       "heaviest sources first, the heaviest on whole warps, by the per-source "
                                       "costs the earlier builds recorded); e2e: a fresh mesh every step with the "
-                                      "default schedule, ordered by a K/10 probe build inside the timed region"),
+                                      "default options (no cost record yet: vertex order, the warps that are "
+                                      "left with one running lane adopt it)"),
             "build_s": total_ms_max / args.steps / 1e3,
             "kernel_ms_per_step": statistics.mean(kern),
             "roofline": roofline_figures(st, peaks, fma_rate()),
@@ -1265,7 +1266,8 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_max / args.steps,
                     "breakdown_ms_mean": {k: round(statistics.mean(v), 2) for k, v in parts.items() if v},
-                    "note": "build_call includes the K/10 probe build that orders a fresh mesh's sources"},
+                    "note": "build_call = the svg_build call's wall time (host set-up, device build, CSR "
+                            "allocation); build_device = its CUDA-event time"},
             "gpu_launches": launches,
             "autotune": tuned,
             "coop": {"sources": st["coop_sources"], "warps": st["coop_warps"]},
