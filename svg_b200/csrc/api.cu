@@ -152,10 +152,18 @@ void upload_mesh(svg_mesh* m) {
     const HostMesh& H = m->h;
     cudaStream_t st = lib_stream();
     MeshDev& D = m->d;
-    D.he = dev_alloc_n<HeRec>((size_t)H.ne);
-    D.geo = dev_alloc_n<HeGeo>((size_t)H.ne);
-    D.vr = dev_alloc_n<VertRec>((size_t)H.nv);
-    D.pos = dev_alloc_n<double>(3 * (size_t)H.nv);
+    auto al256 = [](size_t x) { return (x + 255) / 256 * 256; };
+    // one block, half-edge records first: the records a window step reads
+    // form one contiguous range (an L2 access-policy window can cover it)
+    const size_t b_he = al256(sizeof(HeRec) * (size_t)H.ne), b_geo = al256(sizeof(HeGeo) * (size_t)H.ne),
+                 b_vr = al256(sizeof(VertRec) * (size_t)H.nv), b_pos = al256(sizeof(double) * 3 * (size_t)H.nv);
+    char* blk = static_cast<char*>(dev_alloc(b_he + b_geo + b_vr + b_pos));
+    D.block = blk;
+    D.block_bytes = b_he + b_geo + b_vr + b_pos;
+    D.he = reinterpret_cast<HeRec*>(blk);
+    D.geo = reinterpret_cast<HeGeo*>(blk + b_he);
+    D.vr = reinterpret_cast<VertRec*>(blk + b_he + b_geo);
+    D.pos = reinterpret_cast<double*>(blk + b_he + b_geo + b_vr);
     SVG_CUDA(cudaMemcpyAsync(D.he, H.he.data(), sizeof(HeRec) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.geo, H.geo.data(), sizeof(HeGeo) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.vr, H.vr.data(), sizeof(VertRec) * (size_t)H.nv, cudaMemcpyHostToDevice, st));
@@ -276,10 +284,7 @@ svg_status svg_mesh_upload(svg_mesh* m) {
 
 void svg_mesh_free(svg_mesh* m) {
     if (!m) return;
-    dev_free(m->d.he);
-    dev_free(m->d.geo);
-    dev_free(m->d.vr);
-    dev_free(m->d.pos);
+    dev_free(m->d.block);
     delete m;
 }
 

@@ -57,6 +57,8 @@ struct DevBuf {
 
 struct MeshDev {
     bool uploaded = false;
+    void* block = nullptr;   // one allocation holding he, geo, vr, pos in that order
+    size_t block_bytes = 0;
     int32_t nv = 0, nf = 0, ne = 0;
     HeRec* he = nullptr;
     HeGeo* geo = nullptr;

@@ -44,7 +44,12 @@
 #endif
 // 1: peek() prefetches into L1 the face records the next window step reads
 #ifndef SVG_FACE_PREFETCH
-#define SVG_FACE_PREFETCH 1
+#define SVG_FACE_PREFETCH 0
+#endif
+// 1: the one-thread sifts prefetch keys only and re-read the moved entries
+// (fewer registers); 0: they prefetch whole entries (fewer round trips to L1)
+#ifndef SVG_KEYS_ONLY_SIFT
+#define SVG_KEYS_ONLY_SIFT 1
 #endif
 
 namespace svgb {
@@ -530,37 +535,55 @@ struct LaneT {
             if (lane < m) H[cur >> lane] = e;
             H[cur >> m] = x;
             __syncwarp();
-            return;
-        }
-        // keys of the first four ancestors in one round trip; the moved
-        // entries are read again (their sectors were just fetched) before
-        // each is written one level down
-        double ak[4];
+        } else {
+#if SVG_KEYS_ONLY_SIFT
+            // keys of the first four ancestors in one round trip; the moved
+            // entries are read again (their sectors were just fetched) before
+            // each is written one level down
+            double ak[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) ak[j] = (cur >> (j + 1)) > 0 ? H[cur >> (j + 1)].key : 0.0;
-        int m = 0;
+            for (int j = 0; j < 4; ++j) ak[j] = (cur >> (j + 1)) > 0 ? H[cur >> (j + 1)].key : 0.0;
+            int m = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (m == j && (cur >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
-        T mv[4];
+            for (int j = 0; j < 4; ++j)
+                if (m == j && (cur >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
+            T mv[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (j < m) mv[j] = H[cur >> (j + 1)];
+            for (int j = 0; j < 4; ++j)
+                if (j < m) mv[j] = H[cur >> (j + 1)];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (j < m) H[cur >> j] = mv[j];
-        int c = cur >> m;
-        if (m == 4) {
-            for (;;) {
-                const int p = c >> 1;
-                if (p == 0) break;
-                const T pe = H[p];
-                if (!(pe.key > x.key)) break;
-                H[c] = pe;
-                c = p;
+            for (int j = 0; j < 4; ++j)
+                if (j < m) H[cur >> j] = mv[j];
+#else
+            // the first four ancestors in one round trip (they are what the level-
+            // by-level loop would read: a move only writes below the next
+            // ancestor); the moves over them are counted with the same stop rule
+            // and written predicated
+            T anc[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if ((cur >> (j + 1)) > 0) anc[j] = H[cur >> (j + 1)];
+            int m = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (m == j && (cur >> (j + 1)) > 0 && anc[j].key > x.key) m = j + 1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j < m) H[cur >> j] = anc[j];
+#endif
+            int c = cur >> m;
+            if (m == 4) {
+                for (;;) {
+                    const int p = c >> 1;
+                    if (p == 0) break;
+                    const T pe = H[p];
+                    if (!(pe.key > x.key)) break;
+                    H[c] = pe;
+                    c = p;
+                }
             }
+            H[c] = x;
         }
-        H[c] = x;
     }
 
     // Push (PriorityQueue.cuh:48-67).
@@ -642,6 +665,7 @@ struct LaneT {
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
+#if SVG_KEYS_ONLY_SIFT
             const double a = H[l].key, b = H[l + 1].key;
             const int g = cur << 2;
             double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
@@ -660,6 +684,24 @@ struct LaneT {
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             cur = mv2 ? c2 : (mv1 ? c1 : cur);
+#else
+            const T a = H[l], b = H[l + 1];
+            const int g = cur << 2;
+            T q0, q1, q2, q3;
+            if (g <= n) { q0 = H[g]; q1 = H[g + 1]; q2 = H[g + 2]; q3 = H[g + 3]; }
+            const int k1 = (l + 1 <= n && !(a.key < b.key)) ? 1 : 0;
+            const T e1 = k1 ? b : a;
+            const bool mv1 = e1.key < last.key;
+            const int c1 = l + k1;
+            const int l2 = c1 << 1;
+            const T a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
+            const int k2 = (l2 + 1 <= n && !(a2.key < b2.key)) ? 1 : 0;
+            const T e2 = k2 ? b2 : a2;
+            const bool mv2 = mv1 && l2 <= n && e2.key < last.key;
+            if (mv1) H[cur] = e1;
+            if (mv2) H[c1] = e2;
+            cur = mv2 ? l2 + k2 : (mv1 ? c1 : cur);
+#endif
             if (!mv2) break;
         }
         return cur;
