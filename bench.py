@@ -1154,7 +1154,7 @@ def main():
         kw = dict(source_begin=sb, source_end=se) if shard else {}
         best, best_ms = svg.autotune(max_trials=16, **kw)
         tuned = {"params": {k: best[k] for k in ("coop_sources", "coop_warps", "blocks", "vote_wait",
-                                                 "heavy_waves", "heap_factor")},
+                                                 "heavy_waves", "heap_factor", "coop_tail")},
                  "tuned_build_ms": best_ms, "tuning_s": time.perf_counter() - t0}
     for _ in range(args.warmup):
         timed_build()

@@ -103,7 +103,8 @@ typedef struct svg_build_opts {
     int32_t source_end;       /* 0,0 = all vertices */
     int32_t coop_sources;     /* batched, with a heaviest-first order: this many of the heaviest sources are
                                  each run by a whole warp (warp-cooperative heap and table operations), the
-                                 rest one per lane; -1 automatic, 0 none */
+                                 rest one per lane; -1 automatic (those whose cost exceeds a lane's average
+                                 share), 0 none (the default) */
     int32_t coop_warps;       /* warps that run them (0 automatic) */
     int32_t vote_wait;        /* batched: most loop iterations a lane waits for the warp's vote to pick its
                                  kind of step (0 = 8) */

@@ -632,6 +632,7 @@ svg_build_opts effective_options(const svg_mesh* m, const svg_build_opts& o) {
                 e.heavy_waves = t.opts.heavy_waves;
                 e.heap_factor = t.opts.heap_factor;
                 e.blocks = t.opts.blocks;
+                e.coop_tail = t.opts.coop_tail;
             }
     }
     if (e.vote_wait <= 0) e.vote_wait = 8;
@@ -1136,8 +1137,9 @@ svg_status run_autotune(svg_mesh* m, const svg_build_opts& in, int32_t max_trial
     svg_build_opts base = in;
     base.autotune = 0;
     if (base.heavy_first == 0) base.heavy_first = 1;
-    base.coop_sources = -1;
+    base.coop_sources = 0;
     base.coop_warps = 0;
+    base.coop_tail = 1;
     base.vote_wait = 8;
     base.heavy_waves = 2;
     base.heap_factor = 3;
@@ -1167,7 +1169,6 @@ svg_status run_autotune(svg_mesh* m, const svg_build_opts& in, int32_t max_trial
     trial(base);                   // records the per-source costs at this K (the work order)
     double best_ms = trial(base);  // the defaults, timed with that order
     svg_build_opts best = base;
-    const int32_t n_auto = last.coop_sources;
     auto consider = [&](const svg_build_opts& o) {
         if (trials >= max_trials) return;
         const double ms = trial(o);
@@ -1176,9 +1177,16 @@ svg_status run_autotune(svg_mesh* m, const svg_build_opts& in, int32_t max_trial
             best = o;
         }
     };
-    // threads per source: how many of the heaviest sources run on whole warps
-    for (int32_t n : {0, n_auto / 2, n_auto * 2, n_auto * 4}) {
-        if (n == n_auto || (n == 0 && n_auto == 0) || (n > 0 && n == n_auto / 2 && n_auto < 2)) continue;
+    // threads per source: the heaviest sources on whole warps, the automatic
+    // count (sources above a lane's average share) and half and twice it
+    {
+        svg_build_opts o = best;
+        o.coop_sources = -1;
+        consider(o);
+    }
+    const int32_t n_auto = last.coop_sources;
+    for (int32_t n : {n_auto / 2, n_auto * 2}) {
+        if (n <= 0) continue;
         svg_build_opts o = best;
         o.coop_sources = n;
         o.coop_warps = std::max(1, n / 2);
@@ -1219,6 +1227,11 @@ svg_status run_autotune(svg_mesh* m, const svg_build_opts& in, int32_t max_trial
     for (int32_t f : {2, 4}) {
         svg_build_opts o = best;
         o.heap_factor = f;
+        consider(o);
+    }
+    {  // the drained-queue adoption off
+        svg_build_opts o = best;
+        o.coop_tail = 0;
         consider(o);
     }
     bool found = false;
