@@ -115,6 +115,11 @@ typedef struct svg_build_opts {
                                  this K (if any) in place of the fields above and of blocks */
     int32_t coop_tail;        /* batched: 1 (default) = once the work queue is drained, a warp left with one
                                  running lane finishes that lane's source on all 32 threads; 0 = off */
+    int32_t graph;            /* batched: 1 = the build's device work (memsets, window propagation, offsets
+                                 scan, emission, copies into the graph's buffers) is captured in a CUDA graph
+                                 kept with the mesh, and later builds of the mesh with the same options
+                                 replay it (one launch, no host round trip); a replay whose sources outgrow
+                                 the captured sizes falls back to the ordinary build */
 } svg_build_opts;
 
 typedef struct svg_build_stats {
@@ -138,6 +143,7 @@ typedef struct svg_build_stats {
     int64_t scratch_bytes;    /* device scratch held by the build */
     int32_t coop_sources;     /* sources run by whole warps */
     int32_t coop_warps;       /* warps that ran them */
+    int32_t graph_replayed;   /* 1: this build was a replay of the mesh's captured graph (opts.graph) */
 } svg_build_stats;
 
 void svg_build_opts_default(svg_build_opts* o);

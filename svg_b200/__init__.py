@@ -57,7 +57,7 @@ class BuildOptions(C.Structure):
         ("source_begin", C.c_int32), ("source_end", C.c_int32),
         ("coop_sources", C.c_int32), ("coop_warps", C.c_int32), ("vote_wait", C.c_int32),
         ("heavy_waves", C.c_int32), ("heap_factor", C.c_int32), ("autotune", C.c_int32),
-        ("coop_tail", C.c_int32),
+        ("coop_tail", C.c_int32), ("graph", C.c_int32),
     ]
 
 
@@ -70,6 +70,7 @@ class BuildStats(C.Structure):
         ("ref_overflow_sources", C.c_int32), ("watchdog_sources", C.c_int32),
         ("undefined_sources", C.c_int32), ("retried_sources", C.c_int32), ("launches", C.c_int32),
         ("scratch_bytes", C.c_int64), ("coop_sources", C.c_int32), ("coop_warps", C.c_int32),
+        ("graph_replayed", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -618,6 +618,54 @@ int ilog2_ceil(int64_t x) {
 
 }  // namespace
 
+// ------------------------------------------------------- build as a graph
+//
+// A batched build whose sources all fit the first pass (no retry) and whose
+// candidate pool was large enough can be replayed: the device work is one
+// sequence of memsets, k_ich_batched, the offsets scan, k_emit and the copies
+// of the CSR and per-source counters into the graph's own buffers, over
+// buffers whose sizes the first build fixed.  It is captured once, kept with
+// the mesh, and launched as one graph by later builds with the same options;
+// only the copies' destinations change from launch to launch.  A replay reads
+// back a status block (retry count, candidate pool use, edge count, counters)
+// and falls back to the ordinary build if the sizes no longer hold.
+struct BuildGraph {
+    svg_build_opts opts{};
+    Layout lay;
+    void* arena = nullptr;
+    int32_t nv = 0, nsrc = 0, sb = 0, se = 0;
+    int64_t nnz = 0, cand_cap = 0;
+    int32_t coop_n = 0, coop_warps = 0;
+    int64_t scratch_bytes = 0;
+    bool with_paths = false;
+    DevBuf order, misc, cand, candstart, stats, off, adj, dist, paths, tmp;
+    int32_t* d_retry_n = nullptr;
+    unsigned long long* d_acc = nullptr;  // acc[0..7], cand_used at acc[8]
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t cp_off{}, cp_adj{}, cp_dist{}, cp_paths{}, cp_stats{};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    ~BuildGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+// Options that decide a build's device work (all but the graph switch itself).
+bool same_build_options(const svg_build_opts& a, const svg_build_opts& b) {
+    return a.K == b.K && a.split_coef == b.split_coef && a.vert_coef == b.vert_coef &&
+           a.win_queue_cap == b.win_queue_cap && a.pseudo_queue_cap == b.pseudo_queue_cap && a.mode == b.mode &&
+           a.threads_per_block == b.threads_per_block && a.blocks == b.blocks && a.with_paths == b.with_paths &&
+           a.heavy_first == b.heavy_first && a.hbm_budget == b.hbm_budget && a.source_begin == b.source_begin &&
+           a.source_end == b.source_end && a.coop_sources == b.coop_sources && a.coop_warps == b.coop_warps &&
+           a.vote_wait == b.vote_wait && a.heavy_waves == b.heavy_waves && a.heap_factor == b.heap_factor &&
+           a.coop_tail == b.coop_tail;
+}
+}  // namespace
+
 namespace {
 // Options a build runs with: the caller's, or, with autotune set, the
 // launch parameters svg_build_autotune cached on the mesh for this K.
@@ -642,9 +690,250 @@ svg_build_opts effective_options(const svg_mesh* m, const svg_build_opts& o) {
 }
 }  // namespace
 
+namespace {
+// Flag tallies of a finished build; per-source costs kept on the mesh for
+// the next build's order.
+void record_counts(svg_mesh* m, svg_graph* g, int32_t K, int32_t sb, int32_t se, bool plain) {
+    const int32_t nv = g->nv;
+    svg_build_stats& S = g->stats;
+    std::vector<int32_t> fl((size_t)nv);
+    SVG_CUDA(cudaMemcpy(fl.data(), g->st_flags, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
+    if (!plain) {
+        std::vector<int32_t> w((size_t)nv);
+        SVG_CUDA(cudaMemcpy(w.data(), g->st_windows, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
+        if (m->cost_K != K || (int32_t)m->cost.size() != nv) {
+            m->cost.assign((size_t)nv, 0);
+            m->cost_K = K;
+            m->cost_probe = false;
+        }
+        for (int32_t v = sb; v < se; ++v) m->cost[(size_t)v] = w[(size_t)v];
+        if (sb == 0 && se == nv) m->cost_probe = false;
+    }
+    for (int32_t f : fl) {
+        if (f & 1) ++S.queue_drop_sources;
+        if (f & 2) ++S.ref_overflow_sources;
+        if (f & 4) ++S.watchdog_sources;
+        if (f & 8) ++S.undefined_sources;
+    }
+}
+
+// A replay of the mesh's captured build: false (nothing of g kept) when
+// there is none for these options, the lane scratch has moved, or the
+// sources no longer fit the captured sizes.
+bool replay_graph(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
+    BuildGraph* bg = m->build_graph.get();
+    if (!bg || !same_build_options(bg->opts, o)) return false;
+    if (!(g_arena[0].layout == bg->lay) || g_arena[0].buf.p != bg->arena) return false;
+    cudaStream_t st = lib_stream();
+    const int32_t nv = bg->nv;
+    const size_t E = (size_t)std::max<int64_t>(bg->nnz, 1);
+    g->nv = nv;
+    g->K = o.K;
+    g->with_paths = bg->with_paths;
+    g->st_windows = dev_alloc_n<int32_t>((size_t)nv * 3);
+    g->st_maxq = g->st_windows + nv;
+    g->st_flags = g->st_maxq + nv;
+    g->off = dev_alloc_n<int64_t>((size_t)nv + 1);
+    g->adj = dev_alloc_n<int32_t>(E);
+    g->dist = dev_alloc_n<double>(E);
+    if (g->with_paths) g->paths = dev_alloc(sizeof(PathEnd) * E);
+    const auto D2D = cudaMemcpyDeviceToDevice;
+    SVG_CUDA(cudaGraphExecMemcpyNodeSetParams1D(bg->exec, bg->cp_off, g->off, bg->off.p, sizeof(int64_t) * ((size_t)nv + 1), D2D));
+    SVG_CUDA(cudaGraphExecMemcpyNodeSetParams1D(bg->exec, bg->cp_adj, g->adj, bg->adj.p, sizeof(int32_t) * E, D2D));
+    SVG_CUDA(cudaGraphExecMemcpyNodeSetParams1D(bg->exec, bg->cp_dist, g->dist, bg->dist.p, sizeof(double) * E, D2D));
+    if (g->with_paths)
+        SVG_CUDA(cudaGraphExecMemcpyNodeSetParams1D(bg->exec, bg->cp_paths, g->paths, bg->paths.p, sizeof(PathEnd) * E, D2D));
+    SVG_CUDA(cudaGraphExecMemcpyNodeSetParams1D(bg->exec, bg->cp_stats, g->st_windows, bg->stats.p,
+                                                 sizeof(int32_t) * 3 * (size_t)nv, D2D));
+    cudaEvent_t e0, e1;
+    SVG_CUDA(cudaEventCreate(&e0));
+    SVG_CUDA(cudaEventCreate(&e1));
+    SVG_CUDA(cudaEventRecord(e0, st));
+    SVG_CUDA(cudaGraphLaunch(bg->exec, st));
+    SVG_CUDA(cudaEventRecord(e1, st));
+    int32_t retry_n = 0;
+    unsigned long long acc[9] = {0};
+    int64_t nnz = 0;
+    SVG_CUDA(cudaMemcpyAsync(&retry_n, bg->d_retry_n, sizeof(retry_n), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaMemcpyAsync(acc, bg->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaMemcpyAsync(&nnz, bg->off.as<int64_t>() + nv, sizeof(nnz), cudaMemcpyDeviceToHost, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f, ms_ich = 0.f, ms_emit = 0.f;
+    SVG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    SVG_CUDA(cudaEventElapsedTime(&ms_ich, bg->ev[0], bg->ev[1]));
+    SVG_CUDA(cudaEventElapsedTime(&ms_emit, bg->ev[2], bg->ev[3]));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (retry_n != 0 || (int64_t)acc[8] > bg->cand_cap || nnz != bg->nnz) {
+        free_graph_device(g);
+        return false;
+    }
+    g->nnz = nnz;
+    svg_build_stats& S = g->stats;
+    S = svg_build_stats{};
+    S.ms_ich = ms_ich;
+    S.ms_emit = ms_emit;
+    S.ms_total = ms;
+    S.windows = (int64_t)acc[0];
+    S.windows_generated = (int64_t)acc[1];
+    S.pseudo_sources = (int64_t)acc[2];
+    S.max_win_queue = (int32_t)acc[3];
+    S.max_pseudo_queue = (int32_t)acc[4];
+    S.edges = nnz;
+    S.sources = bg->nsrc;
+    S.launches = 1;
+    S.scratch_bytes = bg->scratch_bytes;
+    S.coop_sources = bg->coop_n;
+    S.coop_warps = bg->coop_warps;
+    S.graph_replayed = 1;
+    record_counts(m, g, o.K, bg->sb, bg->se, false);
+    return true;
+}
+
+struct CapturePlan {
+    LaneConfig C;
+    PhaseOut O;
+    int blocks = 0, tpb = 0;
+    size_t coop_smem = 0;
+    const int32_t* d_order = nullptr;
+    int32_t nsrc = 0, nv = 0, sb = 0, se = 0;
+    int64_t cap = 0, nnz = 0;
+    size_t tmp_bytes = 0, misc_bytes = 0, retry_bytes = 0;
+    int eb = 0, wpb = 0, smax = 32;
+    size_t emit_smem = 0;
+    bool with_paths = false;
+    Layout lay;
+    int64_t scratch_bytes = 0;
+    int32_t coop_n = 0, coop_warps = 0;
+};
+
+// Capture the device work of the build just finished (plan P, result g) as a
+// graph over buffers of its own, kept with the mesh.  g's buffers stand in as
+// the copies' destinations until a replay retargets them.
+void capture_graph(svg_mesh* m, const svg_build_opts& o, const CapturePlan& P, svg_graph* g) {
+    auto bg = std::make_shared<BuildGraph>();
+    cudaStream_t st = lib_stream();
+    const int32_t nv = P.nv;
+    const size_t E = (size_t)std::max<int64_t>(P.nnz, 1);
+    bg->opts = o;
+    bg->lay = P.lay;
+    bg->arena = g_arena[0].buf.p;
+    bg->nv = nv;
+    bg->nsrc = P.nsrc;
+    bg->sb = P.sb;
+    bg->se = P.se;
+    bg->nnz = P.nnz;
+    bg->cand_cap = P.cap;
+    bg->coop_n = P.coop_n;
+    bg->coop_warps = P.coop_warps;
+    bg->scratch_bytes = P.scratch_bytes;
+    bg->with_paths = P.with_paths;
+    bg->order.reserve(sizeof(int32_t) * (size_t)P.nsrc);
+    bg->misc.reserve(P.misc_bytes);
+    bg->cand.reserve(sizeof(Cand) * (size_t)P.cap);
+    bg->candstart.reserve(sizeof(int64_t) * ((size_t)nv + 1));
+    bg->stats.reserve(sizeof(int32_t) * 3 * (size_t)nv);
+    bg->off.reserve(sizeof(int64_t) * ((size_t)nv + 1));
+    bg->adj.reserve(sizeof(int32_t) * E);
+    bg->dist.reserve(sizeof(double) * E);
+    if (P.with_paths) bg->paths.reserve(sizeof(PathEnd) * E);
+    bg->tmp.reserve(P.tmp_bytes + 16);
+    SVG_CUDA(cudaMemcpyAsync(bg->order.p, P.d_order, sizeof(int32_t) * (size_t)P.nsrc, cudaMemcpyDeviceToDevice, st));
+    SVG_CUDA(cudaStreamSynchronize(st));
+    // the misc block laid out as the ordinary build lays it out
+    char* mp = bg->misc.as<char>();
+    int32_t* d_work = reinterpret_cast<int32_t*>(mp);
+    bg->d_retry_n = d_work + 1;
+    bg->d_acc = reinterpret_cast<unsigned long long*>(mp + 64);
+    int32_t* d_cand_n = reinterpret_cast<int32_t*>(mp + 256 + P.retry_bytes);
+    int32_t* d_deg = d_cand_n + align_up(sizeof(int32_t) * ((size_t)nv + 1)) / sizeof(int32_t);
+    int32_t* st_base = bg->stats.as<int32_t>();
+    PhaseOut O = P.O;
+    O.order = bg->order.as<int32_t>();
+    O.work = d_work;
+    O.retry_n = bg->d_retry_n;
+    O.retry = reinterpret_cast<int32_t*>(mp + 256);
+    O.cand = bg->cand.as<Cand>();
+    O.cand_cap = P.cap;
+    O.cand_start = bg->candstart.as<int64_t>();
+    O.cand_used = bg->d_acc + 8;
+    O.cand_n = d_cand_n;
+    O.deg = d_deg;
+    O.st_windows = st_base;
+    O.st_maxq = st_base + nv;
+    O.st_flags = st_base + 2 * (size_t)nv;
+    O.acc = bg->d_acc;
+    O.coop_work = d_work + 4;
+    EmitParams Em{};
+    Em.M = P.C.M;
+    Em.K = P.C.K;
+    Em.nv = nv;
+    Em.order = O.order;
+    Em.nsrc = P.nsrc;
+    Em.cand = O.cand;
+    Em.cand_start = O.cand_start;
+    Em.cand_n = d_cand_n;
+    Em.off = bg->off.as<int64_t>();
+    Em.adj = bg->adj.as<int32_t>();
+    Em.dist = bg->dist.as<double>();
+    Em.path = P.with_paths ? bg->paths.as<PathEnd>() : nullptr;
+    Em.st_flags = O.st_flags;
+    Em.smax = P.smax;
+    for (auto& e : bg->ev) SVG_CUDA(cudaEventCreate(&e));
+    cudaStream_t cs;
+    SVG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    try {
+        SVG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        SVG_CUDA(cudaEventRecordWithFlags(bg->ev[0], cs, cudaEventRecordExternal));
+        SVG_CUDA(cudaMemsetAsync(bg->misc.p, 0, P.misc_bytes, cs));
+        SVG_CUDA(cudaMemsetAsync(bg->stats.p, 0, sizeof(int32_t) * 3 * (size_t)nv, cs));
+        k_ich_batched<<<P.blocks, P.tpb, P.coop_smem, cs>>>(P.C, O);
+        SVG_CUDA(cudaEventRecordWithFlags(bg->ev[1], cs, cudaEventRecordExternal));
+        size_t tb = P.tmp_bytes;
+        SVG_CUDA(cub::DeviceScan::ExclusiveSum(bg->tmp.p, tb, d_deg, bg->off.as<int64_t>(), nv + 1, cs));
+        SVG_CUDA(cudaEventRecordWithFlags(bg->ev[2], cs, cudaEventRecordExternal));
+        k_emit<<<P.eb, P.wpb * 32, P.emit_smem, cs>>>(Em);
+        SVG_CUDA(cudaEventRecordWithFlags(bg->ev[3], cs, cudaEventRecordExternal));
+        SVG_CUDA(cudaStreamEndCapture(cs, &graph));
+    } catch (...) {
+        cudaStreamEndCapture(cs, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        cudaGetLastError();
+        throw;
+    }
+    cudaStreamDestroy(cs);
+    bg->graph = graph;
+    // the captured sequence is one chain: its last node precedes the copies
+    size_t n = 0;
+    SVG_CUDA(cudaGraphGetNodes(graph, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    SVG_CUDA(cudaGraphGetNodes(graph, nodes.data(), &n));
+    cudaGraphNode_t leaf = nullptr;
+    for (auto nd : nodes) {
+        size_t d = 0;
+        SVG_CUDA(cudaGraphNodeGetDependentNodes(nd, nullptr, &d));
+        if (d == 0) leaf = nd;
+    }
+    if (!leaf) throw SvgError{SVG_ERR_STATE, "graph capture: no last node"};
+    const auto D2D = cudaMemcpyDeviceToDevice;
+    SVG_CUDA(cudaGraphAddMemcpyNode1D(&bg->cp_off, graph, &leaf, 1, g->off, bg->off.p, sizeof(int64_t) * ((size_t)nv + 1), D2D));
+    SVG_CUDA(cudaGraphAddMemcpyNode1D(&bg->cp_adj, graph, &leaf, 1, g->adj, bg->adj.p, sizeof(int32_t) * E, D2D));
+    SVG_CUDA(cudaGraphAddMemcpyNode1D(&bg->cp_dist, graph, &leaf, 1, g->dist, bg->dist.p, sizeof(double) * E, D2D));
+    if (P.with_paths)
+        SVG_CUDA(cudaGraphAddMemcpyNode1D(&bg->cp_paths, graph, &leaf, 1, g->paths, bg->paths.p, sizeof(PathEnd) * E, D2D));
+    SVG_CUDA(cudaGraphAddMemcpyNode1D(&bg->cp_stats, graph, &leaf, 1, g->st_windows, bg->stats.p,
+                                      sizeof(int32_t) * 3 * (size_t)nv, D2D));
+    SVG_CUDA(cudaGraphInstantiate(&bg->exec, graph, 0));
+    m->build_graph = bg;
+}
+}  // namespace
+
 svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     const svg_build_opts o = effective_options(m, o_in);
     upload_mesh(m);
+    if (o.graph && o.mode != SVG_BUILD_PLAIN && replay_graph(m, o, g)) return SVG_OK;
     cudaStream_t st = lib_stream();
     const HostMesh& H = m->h;
     const int32_t nv = H.nv;
@@ -751,6 +1040,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     // per-build buffers
     DevBuf b_order, b_misc, b_cand, b_candstart;
     int32_t coop_n = 0, coop_warps = 0;
+    // what a capture of this build as a graph needs (see BuildGraph)
+    size_t cap_coop_smem = 0, cap_emit_smem = 0;
+    int cap_eb = 0, cap_wpb = 0, cap_attempts = 0;
+    int64_t cap_pool = 0;
     b_order.reserve(sizeof(int32_t) * (size_t)std::max(nsrc, 1));
     int32_t* d_order = b_order.as<int32_t>();
     bool ordered = false;
@@ -916,6 +1209,9 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
                                               (int)coop_smem));
             k_ich_batched<<<blocks, tpb, coop_smem, st>>>(C, O);
             ++launches;
+            cap_coop_smem = coop_smem;
+            cap_pool = cap;
+            cap_attempts = attempt;
             SVG_CUDA(cudaGetLastError());
             SVG_CUDA(cudaMemcpyAsync(&retry_n, d_retry_n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             unsigned long long used = 0;
@@ -1023,6 +1319,9 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
         int eb = (int)std::min<int64_t>((nsrc + wpb - 1) / wpb, (int64_t)prop.multiProcessorCount * 16);
         k_emit<<<eb, wpb * 32, smem, st>>>(E);
         ++launches;
+        cap_eb = eb;
+        cap_wpb = wpb;
+        cap_emit_smem = smem;
     }
     SVG_CUDA(cudaGetLastError());
     SVG_CUDA(cudaEventRecord(ev[3], st));
@@ -1060,25 +1359,35 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     S.coop_sources = coop_n;
     S.coop_warps = coop_warps;
     (void)t03;
-    // flag tallies; per-source costs kept on the mesh for the next build's order
-    std::vector<int32_t> fl((size_t)nv);
-    SVG_CUDA(cudaMemcpy(fl.data(), g->st_flags, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
-    if (!plain) {
-        std::vector<int32_t> w((size_t)nv);
-        SVG_CUDA(cudaMemcpy(w.data(), g->st_windows, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost));
-        if (m->cost_K != K || (int32_t)m->cost.size() != nv) {
-            m->cost.assign((size_t)nv, 0);
-            m->cost_K = K;
-            m->cost_probe = false;
-        }
-        for (int32_t v = sb; v < se; ++v) m->cost[(size_t)v] = w[(size_t)v];
-        if (sb == 0 && se == nv) m->cost_probe = false;
-    }
-    for (int32_t f : fl) {
-        if (f & 1) ++S.queue_drop_sources;
-        if (f & 2) ++S.ref_overflow_sources;
-        if (f & 4) ++S.watchdog_sources;
-        if (f & 8) ++S.undefined_sources;
+    record_counts(m, g, K, sb, se, plain);
+    if (o.graph && !plain && nsrc > 0 && retry_n == 0 && cap_attempts == 0) {
+        CapturePlan P;
+        P.C = C;
+        P.O = O;
+        P.blocks = blocks;
+        P.tpb = tpb;
+        P.coop_smem = cap_coop_smem;
+        P.d_order = d_order;
+        P.nsrc = nsrc;
+        P.nv = nv;
+        P.sb = sb;
+        P.se = se;
+        P.cap = cap_pool;
+        P.nnz = nnz;
+        P.tmp_bytes = tmp_bytes;
+        P.misc_bytes = misc_bytes;
+        P.retry_bytes = retry_bytes;
+        P.eb = cap_eb;
+        P.wpb = cap_wpb;
+        P.emit_smem = cap_emit_smem;
+        P.smax = 32;
+        while (P.smax < smax_vlimit) P.smax <<= 1;
+        P.with_paths = g->with_paths;
+        P.lay = lay;
+        P.scratch_bytes = scratch_bytes;
+        P.coop_n = coop_n;
+        P.coop_warps = coop_warps;
+        capture_graph(m, o, P, g);
     }
     return SVG_OK;
 }

@@ -12,6 +12,8 @@
 
 namespace svgb {
 
+struct BuildGraph;  // a build captured as a CUDA graph (build.cu)
+
 void set_error(const std::string& msg);
 
 struct CudaFail {
@@ -79,6 +81,9 @@ struct svg_mesh {
     std::vector<int32_t> cost;
     // the costs are a K/10 probe build's stand-in, not a build at cost_K
     bool cost_probe = false;
+    // the last build captured as a CUDA graph (opts.graph), replayed by later
+    // builds with the same options
+    std::shared_ptr<svgb::BuildGraph> build_graph;
     // Launch parameters svg_build_autotune chose, per K.
     struct Tuned {
         int32_t K;

@@ -134,6 +134,36 @@ def test_tail_adoption_keeps_the_graph():
     assert compare_rows(got_off, got, ooff, onodes) == []
 
 
+def test_build_replayed_from_a_captured_cuda_graph_is_identical():
+    """opts.graph: the first build captures its device work as a CUDA graph
+    kept with the mesh, later builds with the same options replay it; every
+    result equals an ordinary build's rows (path ends included), also after
+    another mesh's build has re-laid the lane scratch, and an option change
+    builds the ordinary way."""
+    pos, faces = meshgen.config_mesh(1, 0.3)
+    ref_off, ref_nodes, _, _, _ = gpu_build(pos, faces, 200)
+    m = Mesh.from_arrays(pos, faces)
+    g = SVG()
+    g.AssignMesh(m)
+    g.SetParameters(200)
+    replays = []
+    for i in range(3):
+        st = g.ConstructSVG(graph=1)
+        replays.append(st["graph_replayed"])
+        off, nodes = g.CopySVGToHost()
+        assert compare_rows(off, nodes, ref_off, ref_nodes) == [], i
+        if i == 1:  # another mesh and K re-lay the shared lane scratch
+            other = SVG()
+            other.AssignMesh(Mesh.from_arrays(*meshgen.torus(1.0, 0.35, 30, 20, 0.02, seed=5)))
+            other.SetParameters(40)
+            other.ConstructSVG()
+    assert replays[0] == 0 and replays[1] == 1
+    st = g.ConstructSVG(graph=1, vote_wait=4)  # other options: no replay
+    assert st["graph_replayed"] == 0
+    off, nodes = g.CopySVGToHost()
+    assert compare_rows(off, nodes, ref_off, ref_nodes) == []
+
+
 def test_autotuned_schedule_keeps_the_graph():
     """The tuner's candidates and its choice change the schedule only: the
     tuned build equals a default build bit for bit (the tuner itself also
