@@ -1063,6 +1063,7 @@ def main():
     ap.add_argument("--plain-seconds", type=float, default=30.0)
     ap.add_argument("--record", default="", help="also write the JSON line to this file")
     ap.add_argument("--no-autotune", action="store_true", help="time the default schedule, not the tuned one")
+    ap.add_argument("--no-graph", action="store_true", help="timed builds without the captured CUDA graph")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: N whole builds (weak scaling) instead of one build sharded by source range")
     args = ap.parse_args()
@@ -1134,10 +1135,13 @@ def main():
         flush_l2()
         a = C.c_double()
         L.svg_timer_mark(C.byref(a))
+        # repeated builds of the resident mesh replay the build captured as a
+        # CUDA graph by the first (warm-up) build; the plain form is not captured
+        gr = int(mode == MODE_BATCHED and not args.no_graph)
         if sharded:
-            st = svg.ConstructSVG(mode=mode, source_begin=sb, source_end=se, autotune=int(tune))
+            st = svg.ConstructSVG(mode=mode, source_begin=sb, source_end=se, autotune=int(tune), graph=gr)
         else:
-            st = svg.ConstructSVG(mode=mode, autotune=int(tune))
+            st = svg.ConstructSVG(mode=mode, autotune=int(tune), graph=gr)
         b = C.c_double()
         L.svg_timer_mark(C.byref(b))
         ms = b.value
@@ -1162,7 +1166,7 @@ def main():
     torch.cuda.synchronize()
     clocks = Clocks(smi_index(local))
     clocks.start()
-    times, kern, edges, launches = [], [], 0, 0
+    times, kern, edges, launches, replayed = [], [], 0, 0, 0
     st = None
     for _ in range(args.steps):
         ms, st = timed_build()
@@ -1170,6 +1174,7 @@ def main():
         kern.append(st["ms_total"])
         edges += st["edges"]
         launches += st["launches"]
+        replayed += st["graph_replayed"]
     torch.cuda.synchronize()
     barrier(dist)
     ck = clocks.stop()
@@ -1270,6 +1275,7 @@ def main():
                             "allocation); build_device = its CUDA-event time"},
             "gpu_launches": launches,
             "autotune": tuned,
+            "graph_replayed_steps": replayed,
             "coop": {"sources": st["coop_sources"], "warps": st["coop_warps"]},
             "clocks": ck,
             "flags": {k: st[k] for k in ("queue_drop_sources", "ref_overflow_sources", "watchdog_sources",
