@@ -781,7 +781,7 @@ bool replay_graph(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     S.max_pseudo_queue = (int32_t)acc[4];
     S.edges = nnz;
     S.sources = bg->nsrc;
-    S.launches = 1;
+    S.launches = 3;  // k_ich_batched, the offsets scan and k_emit, in one graph launch
     S.scratch_bytes = bg->scratch_bytes;
     S.coop_sources = bg->coop_n;
     S.coop_warps = bg->coop_warps;
