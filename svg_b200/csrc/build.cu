@@ -26,13 +26,6 @@
 #include "engine.h"
 #include "ich.cuh"
 
-// 1: the batched build asks L2 to keep the mesh resident (an access-policy
-// window over the device mesh, persisting lines, for the process's own
-// context) while the lanes' scratch streams through the rest of L2.
-#ifndef SVG_L2_PERSIST_MESH
-#define SVG_L2_PERSIST_MESH 0
-#endif
-
 // Blocks of 128 lanes the batched kernel is compiled to fit per SM (register
 // budget); 0 = no constraint.
 #ifndef SVG_ICH_MIN_BLOCKS
@@ -1141,27 +1134,6 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     O.coop_work = d_work + 4;
     O.coop_tail = o.coop_tail != 0 ? 1 : 0;
 
-    // The mesh's half-edge and geometry records are read by every window step
-    // of every lane; the lanes' scratch (gigabytes) would evict them from L2.
-    bool persisting = false;
-    if (SVG_L2_PERSIST_MESH && !plain && m->d.block) {
-        int maxp = 0, maxw = 0;
-        SVG_CUDA(cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev));
-        SVG_CUDA(cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev));
-        if (maxp > 0 && maxw > 0) {
-            const size_t win = std::min<size_t>(m->d.block_bytes, (size_t)maxw);
-            SVG_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, std::min<size_t>((size_t)maxp, win)));
-            cudaStreamAttrValue a{};
-            a.accessPolicyWindow.base_ptr = m->d.block;
-            a.accessPolicyWindow.num_bytes = win;
-            a.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)maxp / (double)win);
-            a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-            a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-            SVG_CUDA(cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &a));
-            persisting = true;
-        }
-    }
-
     cudaEvent_t ev[4];
     for (auto& e : ev) SVG_CUDA(cudaEventCreate(&e));
     int launches = 1;  // iota
@@ -1326,12 +1298,6 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     SVG_CUDA(cudaGetLastError());
     SVG_CUDA(cudaEventRecord(ev[3], st));
     SVG_CUDA(cudaStreamSynchronize(st));
-    if (persisting) {  // the stream's later work (queries, other meshes) gets the whole L2 back
-        cudaStreamAttrValue a{};
-        a.accessPolicyWindow.num_bytes = 0;
-        SVG_CUDA(cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &a));
-        SVG_CUDA(cudaCtxResetPersistingL2Cache());
-    }
 
     unsigned long long acc[8] = {0};
     SVG_CUDA(cudaMemcpy(acc, d_acc, sizeof(acc), cudaMemcpyDeviceToHost));
