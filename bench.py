@@ -1064,6 +1064,8 @@ def main():
     ap.add_argument("--record", default="", help="also write the JSON line to this file")
     ap.add_argument("--no-autotune", action="store_true", help="time the default schedule, not the tuned one")
     ap.add_argument("--no-graph", action="store_true", help="timed builds without the captured CUDA graph")
+    ap.add_argument("--e2e-heavy-first", type=int, default=-1,
+                    help="e2e: heavy_first of the fresh-mesh build (-1 = the library default)")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: N whole builds (weak scaling) instead of one build sharded by source range")
     args = ap.parse_args()
@@ -1210,7 +1212,8 @@ def main():
         s2 = SVG()
         s2.AssignMesh(m2)
         s2.SetParameters(K_BUILD, 10, 2)
-        st2 = s2.ConstructSVG(source_begin=sb, source_end=se) if shard else s2.ConstructSVG()
+        kw = {} if args.e2e_heavy_first < 0 else {"heavy_first": args.e2e_heavy_first}
+        st2 = s2.ConstructSVG(source_begin=sb, source_end=se, **kw) if shard else s2.ConstructSVG(**kw)
         t2 = time.perf_counter()
         off, adj, dist_h = s2.csr(out=out_bufs)
         b = C.c_double()

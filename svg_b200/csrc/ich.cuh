@@ -52,6 +52,10 @@
 #ifndef SVG_KEYS_ONLY_SIFT
 #define SVG_KEYS_ONLY_SIFT 0
 #endif
+// 1: the one-thread sift-down reads the keys of three levels per round trip
+#ifndef SVG_SIFT3
+#define SVG_SIFT3 0
+#endif
 
 namespace svgb {
 
@@ -122,7 +126,7 @@ struct LaneConfig {
     int32_t wcap, pcap;      // logical queue capacities: pushes beyond them are dropped (reference)
     int32_t wphys, pphys;    // physical heap capacities (<= logical); exceeding one hands the
                              // source to the retry pass, which runs with physical = logical
-    int32_t wstride, pstride;// heap entries per lane (>= phys + 4, multiple of 4)
+    int32_t wstride, pstride;// heap entries per lane (>= phys + 8, multiple of 4)
     uint32_t vref, sref;     // the reference's table sizes, K*vert_coef and K*split_coef
     int32_t vcap_log2, scap_log2;
     int32_t vlimit, slimit;  // max keys this lane's tables take before kFlagCapacity
@@ -656,7 +660,7 @@ struct LaneT {
     // up while it is smaller than the last element.  The keys of the children
     // and grandchildren of `cur` are loaded together, so two levels cost one
     // dependent round trip (reads past the heap's end stay inside the lane's
-    // array, stride >= cap + 4, and are never used); the moved entries are read
+    // array, stride >= cap + 8, and are never used); the moved entries are read
     // again from the sectors just fetched and written with predicated stores,
     // one exit test per two levels.
     template <class T>
@@ -666,7 +670,44 @@ struct LaneT {
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
-#if SVG_KEYS_ONLY_SIFT
+#if SVG_SIFT3
+            // keys of three levels below cur (2 + 4 + 8) in one round trip
+            // (reads past the heap's end stay inside the lane's array,
+            // stride >= cap + 8, and are never used); the moved entries are
+            // read again from the sectors just fetched
+            const double a = H[l].key, b = H[l + 1].key;
+            const int g = cur << 2, h8 = cur << 3;
+            double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+            if (g <= n) { q0 = H[g].key; q1 = H[g + 1].key; q2 = H[g + 2].key; q3 = H[g + 3].key; }
+            double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0, r4 = 0.0, r5 = 0.0, r6 = 0.0, r7 = 0.0;
+            if (h8 <= n) {
+                r0 = H[h8].key; r1 = H[h8 + 1].key; r2 = H[h8 + 2].key; r3 = H[h8 + 3].key;
+                r4 = H[h8 + 4].key; r5 = H[h8 + 5].key; r6 = H[h8 + 6].key; r7 = H[h8 + 7].key;
+            }
+            const int k1 = (l + 1 <= n && !(a < b)) ? 1 : 0;
+            const bool mv1 = (k1 ? b : a) < last.key;
+            const int c1 = l + k1;
+            const int l2 = c1 << 1;
+            const double a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
+            const int k2 = (l2 + 1 <= n && !(a2 < b2)) ? 1 : 0;
+            const bool mv2 = mv1 && l2 <= n && (k2 ? b2 : a2) < last.key;
+            const int c2 = l2 + k2;
+            const int l3 = c2 << 1;  // = h8 + 4 k1 + 2 k2
+            const double a3 = k1 ? (k2 ? r6 : r4) : (k2 ? r2 : r0);
+            const double b3 = k1 ? (k2 ? r7 : r5) : (k2 ? r3 : r1);
+            const int k3 = (l3 + 1 <= n && !(a3 < b3)) ? 1 : 0;
+            const bool mv3 = mv2 && l3 <= n && (k3 ? b3 : a3) < last.key;
+            const int c3 = l3 + k3;
+            T e1, e2, e3;
+            if (mv1) e1 = H[c1];
+            if (mv2) e2 = H[c2];
+            if (mv3) e3 = H[c3];
+            if (mv1) H[cur] = e1;
+            if (mv2) H[c1] = e2;
+            if (mv3) H[c2] = e3;
+            cur = mv3 ? c3 : (mv2 ? c2 : (mv1 ? c1 : cur));
+            const bool more = mv3;
+#elif SVG_KEYS_ONLY_SIFT
             const double a = H[l].key, b = H[l + 1].key;
             const int g = cur << 2;
             double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
@@ -685,6 +726,7 @@ struct LaneT {
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             cur = mv2 ? c2 : (mv1 ? c1 : cur);
+            const bool more = mv2;
 #else
             const T a = H[l], b = H[l + 1];
             const int g = cur << 2;
@@ -702,8 +744,9 @@ struct LaneT {
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             cur = mv2 ? l2 + k2 : (mv1 ? c1 : cur);
+            const bool more = mv2;
 #endif
-            if (!mv2) break;
+            if (!more) break;
         }
         return cur;
     }
