@@ -56,6 +56,16 @@
 #ifndef SVG_SIFT3
 #define SVG_SIFT3 0
 #endif
+// 1: the free pool slot on top of the lane's free list is kept in a register,
+// so a push does not wait for the list read
+#ifndef SVG_FREE_CACHE
+#define SVG_FREE_CACHE 1
+#endif
+// 1: the vertex ids of the top window's face are loaded before its pop's
+// sift-down, so propagate() issues its table probes with the face loads
+#ifndef SVG_FACE_IDS
+#define SVG_FACE_IDS 1
+#endif
 
 namespace svgb {
 
@@ -322,6 +332,7 @@ struct LaneT {
     __device__ __forceinline__ int32_t* VL() const { return C.vlist + (size_t)lid * C.vlimit; }
     __device__ __forceinline__ SSlot* ST() const { return C.stab + ((size_t)lid << C.scap_log2); }
     int wsize, psize, nfree, nfresh;
+    int ftop;       // WF()[nfree - 1] when nfree > 0 (free-slot cache)
     int vcount, scount;
     uint32_t epoch;
     int source;
@@ -352,6 +363,7 @@ struct LaneT {
         psize = __shfl_sync(kFull, L.psize, o);
         nfree = __shfl_sync(kFull, L.nfree, o);
         nfresh = __shfl_sync(kFull, L.nfresh, o);
+        ftop = __shfl_sync(kFull, L.ftop, o);
         vcount = __shfl_sync(kFull, L.vcount, o);
         scount = __shfl_sync(kFull, L.scount, o);
         epoch = __shfl_sync(kFull, L.epoch, o);
@@ -602,7 +614,19 @@ struct LaneT {
             flags |= kFlagCapacity;
             return;
         }
+#if SVG_FREE_CACHE
+        // the list entry under the cached top is loaded now and used by the
+        // next push, after this push's sift-up
+        int slot;
+        if (nfree > 0) {
+            slot = ftop;
+            if (--nfree > 0) ftop = WF()[nfree - 1];
+        } else {
+            slot = nfresh++;
+        }
+#else
         const int slot = nfree > 0 ? (int)WF()[--nfree] : nfresh++;
+#endif
         WP()[slot] = w.p;
         WinEntry e;
         e.key = w.key;
@@ -757,6 +781,7 @@ struct LaneT {
         const int cur = sift_down2(WH(), n, last);
         WH()[cur] = last;
         WF()[nfree++] = (uint16_t)(top.sb & 0xFFFF);
+        ftop = (int)(top.sb & 0xFFFF);
         if constexpr (kCoop) __syncwarp();
         return top;
     }
@@ -800,6 +825,7 @@ struct LaneT {
     __device__ void begin(int v, bool clear_all) {
         source = v;
         wsize = psize = nfree = nfresh = 0;
+        ftop = 0;
         vcount = scount = 0;
         total = 0;
         flags = 0;
@@ -919,7 +945,9 @@ struct LaneT {
     // All lanes of `amask` call this together and meet at each __syncwarp, so
     // the phases run converged; a lane with nothing to do (live == false, or a
     // boundary edge, or a full table) only predicates its work off.
-    __device__ void propagate(const WinPay& win, int psrc, int birth, bool live, unsigned amask) {
+    // fid: the face's vertex ids (h0.v0, h0.v1, h1.v1) when loaded ahead
+    // (SVG_FACE_IDS), else unused
+    __device__ void propagate(const WinPay& win, int psrc, int birth, bool live, unsigned amask, const int3& fid) {
         const DevMesh& M = C.M;
         const int e0 = win.cross;
         live = live && e0 != -1;
@@ -940,9 +968,15 @@ struct LaneT {
             v2 = ld_apex(M.geo, e0);
             top1 = ld_top(M.geo, e1);
             top2 = ld_top(M.geo, e2);
+#if SVG_FACE_IDS
+            A = fid.x;
+            B = fid.y;
+            Cv = fid.z;
+#else
             A = h0.v0;
             B = h0.v1;
             Cv = h1.v1;
+#endif
             if constexpr (!kCoop) {
                 vfirst(A, hA, kA, dA);
                 vfirst(B, hB, kB, dB);
@@ -1175,6 +1209,7 @@ struct LaneT {
     bool pk_proc;  // process (true) or just drop an outdated entry (false)
     WinEntry pk_w;
     PsEntry pk_p;
+    int pk_cross;  // the top window's half-edge (-1: none or boundary)
 
     // Up to this many outdated tops (pseudo-source reborn since the entry was
     // queued) are popped inside peek() instead of spending a voted step each;
@@ -1232,6 +1267,7 @@ struct LaneT {
         if constexpr (kCoop) {
             // the top window's half-edge, loaded before the probe's round trip
             const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
+            pk_cross = cross;
             ProbeR rw, rp, r2, r3;
             coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pk_w.psrc, wlook),
                         probe_q(VT(), C.vcap_log2, (uint32_t)pk_p.vert, plook), probe_off(), probe_off(), epoch, rw,
@@ -1249,6 +1285,7 @@ struct LaneT {
             // birth probes (its sector is the payload's, read again when the
             // window is popped)
             const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
+            pk_cross = cross;
             if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
             if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
             if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
@@ -1275,11 +1312,21 @@ struct LaneT {
         pay.cross = -1;
         pay.level = 0;
         if (proc) pay = WP()[t.sb & 0xFFFF];  // issued before the sift-down
+        int3 fid = make_int3(0, 0, 0);
+#if SVG_FACE_IDS
+        // the face's vertex ids, also issued before the sift-down (the
+        // half-edge is the payload's, read by peek())
+        if (proc && pk_cross >= 0) {
+            const int4 a0 = __ldg(reinterpret_cast<const int4*>(C.M.he + pk_cross));
+            const int4 a1 = __ldg(reinterpret_cast<const int4*>(C.M.he + nxt(pk_cross)));
+            fid = make_int3(a0.x, a0.y, a1.y);
+        }
+#endif
         wpop();
         __syncwarp(amask);
         const bool live = proc && !(pay.level > C.M.nf);
         if (live) ++windows;
-        propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask);
+        propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask, fid);
         if (live && C.K != -1 && total >= C.K) done = true;
     }
 
