@@ -1264,7 +1264,8 @@ def main():
                            work_order="timed steps: the autotuned schedule (untimed tuning before the warm-up; "
                                       "heaviest sources first, the heaviest on whole warps, by the per-source "
                                       "costs the earlier builds recorded); e2e: a fresh mesh every step with the "
-                                      "default options (no cost record yet: vertex order, the warps that are "
+                                      "default options (no cost record yet: on this mesh, under 4 sources per lane at "
+                                      "K >= 160, a K/10 probe build orders the sources; the warps that are "
                                       "left with one running lane adopt it)"),
             "build_s": total_ms_max / args.steps / 1e3,
             "kernel_ms_per_step": statistics.mean(kern),

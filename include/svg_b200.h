@@ -97,7 +97,8 @@ typedef struct svg_build_opts {
     int32_t with_paths;       /* 1 = also produce the path-end fields of svg_node */
     int32_t heavy_first;      /* batched: order the work queue heaviest first, by the per-source cost of the
                                  mesh's previous build at this K (1), or, lacking one, of a probe build at
-                                 K/10 (2); 0: vertex order */
+                                 K/10 when K >= 160 and a launch's lanes get at most 4 sources each
+                                 (2, the default); 0: vertex order */
     int64_t hbm_budget;       /* bytes of scratch the build may hold (0 = automatic) */
     int32_t source_begin;     /* build rows for sources [source_begin, source_end) only; */
     int32_t source_end;       /* 0,0 = all vertices */

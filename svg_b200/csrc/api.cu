@@ -327,7 +327,7 @@ void svg_build_opts_default(svg_build_opts* o) {
     o->pseudo_queue_cap = 1023;  // PSEUDOWINPQ_SIZE - 1
     o->mode = SVG_BUILD_BATCHED;
     o->with_paths = 1;
-    o->heavy_first = 1;
+    o->heavy_first = 2;  // a K/10 probe orders a fresh mesh's first build when a lane gets few sources
     o->coop_sources = 0;  // measured: no upfront cooperative share is fastest on the benchmark meshes
     o->coop_tail = 1;
 }

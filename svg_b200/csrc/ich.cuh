@@ -53,13 +53,25 @@
 #define SVG_KEYS_ONLY_SIFT 0
 #endif
 // 1: the one-thread sift-down reads the keys of three levels per round trip
+// (measured 2.6 % faster on the 72.9K height field at K = 500, 4 % on the
+// 750K torus)
 #ifndef SVG_SIFT3
-#define SVG_SIFT3 0
+#define SVG_SIFT3 1
 #endif
 // 1: the free pool slot on top of the lane's free list is kept in a register,
 // so a push does not wait for the list read
 #ifndef SVG_FREE_CACHE
 #define SVG_FREE_CACHE 1
+#endif
+// 1: the pseudo-source fan walks load the next half-edge records before the
+// current one's push or table probe
+#ifndef SVG_FAN_PIPE
+#define SVG_FAN_PIPE 1
+#endif
+// 1: propagate() builds, tests and pushes one child window at a time through
+// one copy of the code (fewer live registers)
+#ifndef SVG_SEQ_CHILD
+#define SVG_SEQ_CHILD 1
 #endif
 // 1: the vertex ids of the top window's face are loaded before its pop's
 // sift-down, so propagate() issues its table probes with the face loads
@@ -1056,6 +1068,33 @@ struct LaneT {
         }
         __syncwarp(amask);
 
+#if SVG_SEQ_CHILD
+        // One child at a time through one copy of the code: build, test,
+        // push.  The tests read only the three distances, which a push does
+        // not change, so the heap sees the pushes in the same order.
+#pragma unroll 1
+        for (int c = 0; c < 2; ++c) {
+            const bool left = c == 0;
+            bool keep = left ? keep0 : keep1;
+            NewWin W;
+            if (keep) {
+                // child 0: frame (0,0) -> apex; child 1: apex -> (l0,0)
+                const double f0x = left ? 0.0 : v2.x, f0y = left ? 0.0 : v2.y;
+                const double f1x = left ? v2.x : l0, f1y = left ? v2.y : 0.0;
+                const bool fix0 = !left && both, fix1 = left && both;
+                const double t0 = fix0 ? 1.0 : isect(sx, sy, win.b0, 0.0, f0x, f0y, f1x, f1y);
+                const double t1 = fix1 ? 0.0 : isect(sx, sy, win.b1, 0.0, f0x, f0y, f1x, f1y);
+                const double elen = left ? h1.len : h2.len;
+                build_window(win, left ? h1.twin : h2.twin, elen, t0, t1, f0x, f0y, f1x, f1y, W);
+                keep = left ? valid_window(W, true, dB, dC, dA, elen, top1.x, top1.y)
+                            : valid_window(W, false, dC, dA, dB, elen, top2.x, top2.y);
+            }
+            __syncwarp(amask);
+            if (keep) wpush(W, psrc, birth);
+            __syncwarp(amask);
+        }
+    }
+#else
         NewWin W0, W1;
         if (keep0) {
             const double t0 = isect(sx, sy, win.b0, 0.0, 0.0, 0.0, v2.x, v2.y);
@@ -1075,6 +1114,7 @@ struct LaneT {
         if (keep1) wpush(W1, psrc, birth);
         __syncwarp(amask);
     }
+#endif
 
     // Fan walks of GenSubWinsForPseudoSrcFrom{Window,PseudoSrc}
     // (ICHDevice.cu:821-857, 867-903) with precomputed corner angles.
@@ -1140,6 +1180,39 @@ struct LaneT {
             if (flags & kFlagWatchdog) live = false;
         }
         __syncwarp(amask);
+#if SVG_FAN_PIPE
+        // The same walk with the next face's records loaded before this
+        // face's push, so the two round trips overlap.
+        if (live) {
+            int guard = 0;
+            int se = startEdge;
+            HeRec hs, hw, hn;
+            if (se >= 0) {
+                const int we = nxt(se);
+                hs = ld_he(M.he, se); hw = ld_he(M.he, we); hn = ld_he(M.he, nxt(we));
+            }
+            for (;;) {
+                if (se < 0) {  // the reference reads edges[-1] here
+                    flags |= kFlagUndefined;
+                    break;
+                }
+                NewWin w;
+                finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
+                w.p.cross = hw.twin;
+                w.p.level = plevel + 1;
+                const int nse = hn.twin;
+                const bool more = nse != endEdge;
+                if (more && nse >= 0) {
+                    const int we = nxt(nse);
+                    hs = ld_he(M.he, nse); hw = ld_he(M.he, we); hn = ld_he(M.he, nxt(we));
+                }
+                wpush(w, pv, pbirth);
+                se = nse;
+                if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
+                if (!more) break;
+            }
+        }
+#else
         if (live) {
             int guard = 0;
             do {
@@ -1159,13 +1232,28 @@ struct LaneT {
                 if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
             } while (startEdge != endEdge);
         }
+#endif
         __syncwarp(amask);
         if (live) {
             int start = __ldg(&M.vr[pv].first), cur = start;
             int guard = 0;
+#if SVG_FAN_PIPE
+            // each half-edge record is loaded one iteration ahead, beside the
+            // current neighbour's table probe
+            HeRec hn = ld_he(M.he, cur);
+#endif
             do {
                 if (++guard > 1 << 20) { flags |= kFlagWatchdog; break; }
+#if SVG_FAN_PIPE
+                const HeRec hc = hn;
+                {
+                    int nc = hc.twin;
+                    if (nc != -1) nc = nxt(nc);
+                    if (nc != start && nc != -1) hn = ld_he(M.he, nc);
+                }
+#else
                 HeRec hc = ld_he(M.he, cur);
+#endif
                 int opv = hc.v1;
                 int os = vfind(opv);
                 double od = os < 0 ? DBL_MAX : VT()[os].dist;
