@@ -70,19 +70,19 @@ struct PhaseOut {
 
 template <class LaneType>
 __device__ void record_stats(const LaneType& L, const PhaseOut& O, int v) {
-    O.st_windows[v] = L.windows;
-    O.st_maxq[v] = L.maxw;
+    O.st_windows[v] = L.st_windows();
+    O.st_maxq[v] = L.st_maxw();
     int f = 0;
     if (L.flags & kFlagQueueDrop) f |= 1;
     if (L.flags & kFlagRefOverflow) f |= 2;
     if (L.flags & kFlagWatchdog) f |= 4;
     if (L.flags & kFlagUndefined) f |= 8;
     O.st_flags[v] = f;
-    atomicAdd(&O.acc[0], (unsigned long long)L.windows);
-    atomicAdd(&O.acc[1], (unsigned long long)L.generated);
-    atomicAdd(&O.acc[2], (unsigned long long)L.pseudos);
-    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[3]), (unsigned long long)L.maxw);
-    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[4]), (unsigned long long)L.maxp);
+    atomicAdd(&O.acc[0], (unsigned long long)L.st_windows());
+    atomicAdd(&O.acc[1], (unsigned long long)L.st_generated());
+    atomicAdd(&O.acc[2], (unsigned long long)L.st_pseudos());
+    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[3]), (unsigned long long)L.st_maxw());
+    atomicMax(reinterpret_cast<unsigned long long*>(&O.acc[4]), (unsigned long long)L.st_maxp());
 }
 
 // End of the sources of the lanes in `amask` (they finished in this step):

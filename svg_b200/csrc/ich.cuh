@@ -68,6 +68,11 @@
 #ifndef SVG_FAN_PIPE
 #define SVG_FAN_PIPE 1
 #endif
+// 1: a lane's counters and its cached look at the heap tops live in shared
+// memory (one slot per thread, structure of arrays) instead of registers
+#ifndef SVG_SMEM_STATE
+#define SVG_SMEM_STATE 0
+#endif
 // 1: propagate() builds, tests and pushes one child window at a time through
 // one copy of the code (fewer live registers)
 #ifndef SVG_SEQ_CHILD
@@ -318,6 +323,23 @@ __device__ __forceinline__ ProbeQ probe_off() {
     return q;
 }
 
+#if SVG_SMEM_STATE
+// Per-thread slots (blocks of up to 128 threads) of the lane state that a
+// step touches once or twice: counters and the cached heap tops.
+struct LaneSmem {
+    double wkey[128];
+    int32_t wpsrc[128];
+    uint32_t wsb[128];
+    double pkey[128];
+    int32_t pvert[128];
+    uint32_t plb[128];
+    int32_t cross[128];
+    int32_t windows[128], pseudos[128], generated[128], maxw[128], maxp[128];
+    long long steps[128];
+};
+__shared__ LaneSmem g_lane_smem;
+#endif
+
 template <bool kCoop>
 struct LaneT {
     const LaneConfig& C;
@@ -351,8 +373,29 @@ struct LaneT {
     int src_birth;
     int total;      // totalCalcVertNum
     int flags;
-    int windows, pseudos, generated, maxw, maxp;
-    int64_t steps;
+#if SVG_SMEM_STATE
+    __device__ __forceinline__ int& st_windows() const { return g_lane_smem.windows[threadIdx.x]; }
+    __device__ __forceinline__ int& st_pseudos() const { return g_lane_smem.pseudos[threadIdx.x]; }
+    __device__ __forceinline__ int& st_generated() const { return g_lane_smem.generated[threadIdx.x]; }
+    __device__ __forceinline__ int& st_maxw() const { return g_lane_smem.maxw[threadIdx.x]; }
+    __device__ __forceinline__ int& st_maxp() const { return g_lane_smem.maxp[threadIdx.x]; }
+    __device__ __forceinline__ long long& st_steps() const { return g_lane_smem.steps[threadIdx.x]; }
+#else
+    int windows_, pseudos_, generated_, maxw_, maxp_;
+    long long steps_;
+    __device__ __forceinline__ int& st_windows() { return windows_; }
+    __device__ __forceinline__ int& st_pseudos() { return pseudos_; }
+    __device__ __forceinline__ int& st_generated() { return generated_; }
+    __device__ __forceinline__ int& st_maxw() { return maxw_; }
+    __device__ __forceinline__ int& st_maxp() { return maxp_; }
+    __device__ __forceinline__ long long& st_steps() { return steps_; }
+    __device__ __forceinline__ int st_windows() const { return windows_; }
+    __device__ __forceinline__ int st_pseudos() const { return pseudos_; }
+    __device__ __forceinline__ int st_generated() const { return generated_; }
+    __device__ __forceinline__ int st_maxw() const { return maxw_; }
+    __device__ __forceinline__ int st_maxp() const { return maxp_; }
+    __device__ __forceinline__ long long st_steps() const { return steps_; }
+#endif
 
     // gtid: the thread's global index (one-thread form) or the warp's first
     // thread's (cooperative form: the warp uses that thread's scratch).
@@ -383,12 +426,20 @@ struct LaneT {
         src_birth = __shfl_sync(kFull, L.src_birth, o);
         total = __shfl_sync(kFull, L.total, o);
         flags = __shfl_sync(kFull, L.flags, o);
-        windows = __shfl_sync(kFull, L.windows, o);
-        pseudos = __shfl_sync(kFull, L.pseudos, o);
-        generated = __shfl_sync(kFull, L.generated, o);
-        maxw = __shfl_sync(kFull, L.maxw, o);
-        maxp = __shfl_sync(kFull, L.maxp, o);
-        steps = __shfl_sync(kFull, L.steps, o);
+        // (with SVG_SMEM_STATE both lanes' counters are this thread's slot:
+        // each thread reads its slot, the shuffle syncs, each writes its slot)
+        const int sw = __shfl_sync(kFull, L.st_windows(), o);
+        const int sp = __shfl_sync(kFull, L.st_pseudos(), o);
+        const int sg = __shfl_sync(kFull, L.st_generated(), o);
+        const int smw = __shfl_sync(kFull, L.st_maxw(), o);
+        const int smp = __shfl_sync(kFull, L.st_maxp(), o);
+        const long long sst = __shfl_sync(kFull, L.st_steps(), o);
+        st_windows() = sw;
+        st_pseudos() = sp;
+        st_generated() = sg;
+        st_maxw() = smw;
+        st_maxp() = smp;
+        st_steps() = sst;
         done = __shfl_sync(kFull, (int)L.done, o) != 0;
         pk_valid = false;
     }
@@ -617,7 +668,7 @@ struct LaneT {
 
     // Push (PriorityQueue.cuh:48-67).
     __device__ void wpush(const NewWin& w, int psrc, int birth) {
-        ++generated;  // counts attempts, like numOfWinGen
+        ++st_generated();  // counts attempts, like numOfWinGen
         if (wsize >= C.wcap) {  // PriorityQueue.cuh:53: dropped when full
             flags |= kFlagQueueDrop;
             return;
@@ -645,7 +696,7 @@ struct LaneT {
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
         sift_up(WH(), ++wsize, e);
-        if (wsize > maxw) maxw = wsize;
+        if (wsize > st_maxw()) st_maxw() = wsize;
     }
     // Cooperative sift-down: the 62 nodes 1-5 levels below `cur` are loaded
     // in one round trip (two per thread: node k, k+32 of the subtree in level
@@ -821,7 +872,7 @@ struct LaneT {
             }
             ph(cur) = e;
         }
-        if (psize > maxp) maxp = psize;
+        if (psize > st_maxp()) st_maxp() = psize;
     }
     __device__ PsEntry ppop() {
         PsEntry top = PH()[1];
@@ -841,8 +892,8 @@ struct LaneT {
         vcount = scount = 0;
         total = 0;
         flags = 0;
-        windows = pseudos = generated = maxw = maxp = 0;
-        steps = 0;
+        st_windows() = st_pseudos() = st_generated() = st_maxw() = st_maxp() = 0;
+        st_steps() = 0;
         src_birth = 0;
         done = false;
         pk_valid = false;
@@ -1295,9 +1346,36 @@ struct LaneT {
     bool pk_valid;
     int pk_act;
     bool pk_proc;  // process (true) or just drop an outdated entry (false)
-    WinEntry pk_w;
-    PsEntry pk_p;
-    int pk_cross;  // the top window's half-edge (-1: none or boundary)
+#if SVG_SMEM_STATE
+    __device__ __forceinline__ void set_pk(const WinEntry& w, const PsEntry& p) const {
+        const int t = threadIdx.x;
+        g_lane_smem.wkey[t] = w.key; g_lane_smem.wpsrc[t] = w.psrc; g_lane_smem.wsb[t] = w.sb;
+        g_lane_smem.pkey[t] = p.key; g_lane_smem.pvert[t] = p.vert; g_lane_smem.plb[t] = p.lb;
+    }
+    __device__ __forceinline__ WinEntry pk_w() const {
+        const int t = threadIdx.x;
+        WinEntry w;
+        w.key = g_lane_smem.wkey[t]; w.psrc = g_lane_smem.wpsrc[t]; w.sb = g_lane_smem.wsb[t];
+        return w;
+    }
+    __device__ __forceinline__ PsEntry pk_p() const {
+        const int t = threadIdx.x;
+        PsEntry p;
+        p.key = g_lane_smem.pkey[t]; p.vert = g_lane_smem.pvert[t]; p.lb = g_lane_smem.plb[t];
+        return p;
+    }
+    __device__ __forceinline__ void set_pk_cross(int c) const { g_lane_smem.cross[threadIdx.x] = c; }
+    __device__ __forceinline__ int pk_cross() const { return g_lane_smem.cross[threadIdx.x]; }
+#else
+    WinEntry pkw_;
+    PsEntry pkp_;
+    int pkc_;  // the top window's half-edge (-1: none or boundary)
+    __device__ __forceinline__ void set_pk(const WinEntry& w, const PsEntry& p) { pkw_ = w; pkp_ = p; }
+    __device__ __forceinline__ WinEntry pk_w() const { return pkw_; }
+    __device__ __forceinline__ PsEntry pk_p() const { return pkp_; }
+    __device__ __forceinline__ void set_pk_cross(int c) { pkc_ = c; }
+    __device__ __forceinline__ int pk_cross() const { return pkc_; }
+#endif
 
     // Up to this many outdated tops (pseudo-source reborn since the entry was
     // queued) are popped inside peek() instead of spending a voted step each;
@@ -1339,26 +1417,29 @@ struct LaneT {
             done = true;
             return pk_act = kActDone;
         }
-        if (++steps > C.watchdog) {
+        if (++st_steps() > C.watchdog) {
             flags |= kFlagWatchdog;
             done = true;
             return pk_act = kActDone;
         }
-        pk_w.key = 0.0; pk_w.psrc = 0; pk_w.sb = 0;
-        pk_p.key = 0.0; pk_p.vert = 0; pk_p.lb = 0;
-        if (wsize > 0) pk_w = WH()[1];
-        if (psize > 0) pk_p = PH()[1];
+        WinEntry pw;
+        PsEntry pp;
+        pw.key = 0.0; pw.psrc = 0; pw.sb = 0;
+        pp.key = 0.0; pp.vert = 0; pp.lb = 0;
+        if (wsize > 0) pw = WH()[1];
+        if (psize > 0) pp = PH()[1];
+        set_pk(pw, pp);
         // both birth lookups issued together
-        const bool wlook = wsize > 0 && pk_w.psrc != source;
+        const bool wlook = wsize > 0 && pw.psrc != source;
         const bool plook = psize > 0;
         int wb = src_birth, pb = -1;
         if constexpr (kCoop) {
             // the top window's half-edge, loaded before the probe's round trip
-            const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
-            pk_cross = cross;
+            const int cross = wsize > 0 ? WP()[pw.sb & 0xFFFF].cross : -1;
+            set_pk_cross(cross);
             ProbeR rw, rp, r2, r3;
-            coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pk_w.psrc, wlook),
-                        probe_q(VT(), C.vcap_log2, (uint32_t)pk_p.vert, plook), probe_off(), probe_off(), epoch, rw,
+            coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pw.psrc, wlook),
+                        probe_q(VT(), C.vcap_log2, (uint32_t)pp.vert, plook), probe_off(), probe_off(), epoch, rw,
                         rp, r2, r3);
             if (wlook) wb = rw.slot < 0 ? -1 : rw.head.w;
             if (plook) pb = rp.slot < 0 ? -1 : rp.head.w;
@@ -1367,24 +1448,24 @@ struct LaneT {
             uint32_t hw = 0, hp = 0;
             int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
             double dw = 0.0, dp = 0.0;
-            if (wlook) vfirst(pk_w.psrc, hw, kw, dw);
-            if (plook) vfirst(pk_p.vert, hp, kp, dp);
+            if (wlook) vfirst(pw.psrc, hw, kw, dw);
+            if (plook) vfirst(pp.vert, hp, kp, dp);
             // the top window's half-edge, loaded in the same round trip as the
             // birth probes (its sector is the payload's, read again when the
             // window is popped)
-            const int cross = wsize > 0 ? WP()[pk_w.sb & 0xFFFF].cross : -1;
-            pk_cross = cross;
-            if (wlook) wb = vfinish(pk_w.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
-            if (plook) pb = vfinish(pk_p.vert, hp, kp, dp) < 0 ? -1 : kp.w;
+            const int cross = wsize > 0 ? WP()[pw.sb & 0xFFFF].cross : -1;
+            set_pk_cross(cross);
+            if (wlook) wb = vfinish(pw.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
+            if (plook) pb = vfinish(pp.vert, hp, kp, dp) < 0 ? -1 : kp.w;
             if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
         }
-        const bool wstale = wsize > 0 && (int)(signed char)(pk_w.sb >> 16) != wb;
+        const bool wstale = wsize > 0 && (int)(signed char)(pw.sb >> 16) != wb;
         if (wstale) return pk_act = kActWindow;
-        const bool pstale = psize > 0 && (int)(signed char)(pk_p.lb & 0xFF) != pb;
+        const bool pstale = psize > 0 && (int)(signed char)(pp.lb & 0xFF) != pb;
         if (pstale) return pk_act = kActPseudo;
         pk_proc = true;
-        if (wsize > 0 && (psize == 0 || pk_w.key < pk_p.key)) return pk_act = kActWindow;
-        if (psize > 0 && (wsize == 0 || pk_w.key >= pk_p.key)) return pk_act = kActPseudo;
+        if (wsize > 0 && (psize == 0 || pw.key < pp.key)) return pk_act = kActWindow;
+        if (psize > 0 && (wsize == 0 || pw.key >= pp.key)) return pk_act = kActPseudo;
         flags |= kFlagWatchdog;  // NaN keys: neither branch is taken; the reference spins
         done = true;
         return pk_act = kActDone;
@@ -1395,7 +1476,7 @@ struct LaneT {
     __device__ void act_window(unsigned amask) {
         pk_valid = false;
         const bool proc = pk_proc;
-        const WinEntry t = pk_w;
+        const WinEntry t = pk_w();
         WinPay pay;
         pay.cross = -1;
         pay.level = 0;
@@ -1404,16 +1485,17 @@ struct LaneT {
 #if SVG_FACE_IDS
         // the face's vertex ids, also issued before the sift-down (the
         // half-edge is the payload's, read by peek())
-        if (proc && pk_cross >= 0) {
-            const int4 a0 = __ldg(reinterpret_cast<const int4*>(C.M.he + pk_cross));
-            const int4 a1 = __ldg(reinterpret_cast<const int4*>(C.M.he + nxt(pk_cross)));
+        const int pc = pk_cross();
+        if (proc && pc >= 0) {
+            const int4 a0 = __ldg(reinterpret_cast<const int4*>(C.M.he + pc));
+            const int4 a1 = __ldg(reinterpret_cast<const int4*>(C.M.he + nxt(pc)));
             fid = make_int3(a0.x, a0.y, a1.y);
         }
 #endif
         wpop();
         __syncwarp(amask);
         const bool live = proc && !(pay.level > C.M.nf);
-        if (live) ++windows;
+        if (live) ++st_windows();
         propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask, fid);
         if (live && C.K != -1 && total >= C.K) done = true;
     }
@@ -1421,12 +1503,12 @@ struct LaneT {
     __device__ void act_pseudo(unsigned amask) {
         pk_valid = false;
         const bool proc = pk_proc;
-        const PsEntry t = pk_p;
+        const PsEntry t = pk_p();
         ppop();
         __syncwarp(amask);
         const int level = (int)(t.lb >> 8);
         const bool live = proc && !(level >= C.M.nf);
-        if (live) ++pseudos;
+        if (live) ++st_pseudos();
         gen_sub_wins(t.key, t.vert, level, (int)(signed char)(t.lb & 0xFF), live, amask);
         if (live && C.K != -1 && total >= C.K) done = true;
     }
