@@ -31,6 +31,11 @@
 #ifndef SVG_ICH_MIN_BLOCKS
 #define SVG_ICH_MIN_BLOCKS 0
 #endif
+// the lane hash tables hold 2^SVG_TABLE_SHIFT times the slots of the base
+// sizing below (fewer collisions, each a dependent round trip)
+#ifndef SVG_TABLE_SHIFT
+#define SVG_TABLE_SHIFT 0
+#endif
 #if SVG_ICH_MIN_BLOCKS > 0
 #define SVG_ICH_BOUNDS __launch_bounds__(128, SVG_ICH_MIN_BLOCKS)
 #else
@@ -1010,8 +1015,8 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
     Layout lay;
     lay.wphys = C.wphys;
     lay.pphys = C.pphys;
-    lay.vcap_log2 = std::max(6, ilog2_ceil(2 * ((int64_t)C.vref + 1)));
-    lay.scap_log2 = std::max(8, ilog2_ceil(8 * (int64_t)K));  // split entries reach ~1.6x the vertices
+    lay.vcap_log2 = std::max(6, ilog2_ceil(2 * ((int64_t)C.vref + 1))) + SVG_TABLE_SHIFT;
+    lay.scap_log2 = std::max(8, ilog2_ceil(8 * (int64_t)K)) + SVG_TABLE_SHIFT;  // split entries reach ~1.6x the vertices
     lay.vlimit = (int32_t)(((int64_t)3 << lay.vcap_log2) / 4);
     C.vcap_log2 = lay.vcap_log2;
     C.scap_log2 = lay.scap_log2;

@@ -46,11 +46,12 @@
 #ifndef SVG_FACE_PREFETCH
 #define SVG_FACE_PREFETCH 0
 #endif
-// 1: the one-thread sifts prefetch keys only and re-read the moved entries
-// (234 registers, no spill); 0: they prefetch whole entries (one L1 round trip
-// fewer per move; measured 0.5-2.7 % faster at two blocks per SM)
+// 1: the one-thread sifts prefetch keys only and re-read the moved entries;
+// 0: they prefetch whole entries (one L1 round trip fewer per move).  With the
+// three-level sift-down below, keys only measured 1.3 % faster (the sift-up
+// holds fewer registers)
 #ifndef SVG_KEYS_ONLY_SIFT
-#define SVG_KEYS_ONLY_SIFT 0
+#define SVG_KEYS_ONLY_SIFT 1
 #endif
 // 1: the one-thread sift-down reads the keys of three levels per round trip
 // (measured 2.6 % faster on the 72.9K height field at K = 500, 4 % on the
@@ -59,29 +60,41 @@
 #define SVG_SIFT3 1
 #endif
 // 1: the free pool slot on top of the lane's free list is kept in a register,
-// so a push does not wait for the list read
+// so a push does not wait for the list read (measured 1-1.5 % faster)
 #ifndef SVG_FREE_CACHE
 #define SVG_FREE_CACHE 1
 #endif
 // 1: the pseudo-source fan walks load the next half-edge records before the
-// current one's push or table probe
+// current one's push or table probe (measured 3 % slower: off)
 #ifndef SVG_FAN_PIPE
-#define SVG_FAN_PIPE 1
+#define SVG_FAN_PIPE 0
 #endif
 // 1: a lane's counters and its cached look at the heap tops live in shared
 // memory (one slot per thread, structure of arrays) instead of registers
 #ifndef SVG_SMEM_STATE
 #define SVG_SMEM_STATE 0
 #endif
+// 1: the lane keeps copies of its two heap tops, updated by every push and
+// pop (a pop's sift-down reads the new top anyway), so a look at the tops
+// costs no global round trip
+#ifndef SVG_TOP_CACHE
+#define SVG_TOP_CACHE 1
+#endif
+// 1: the one-thread pseudo-source push climbs with the window push's sift-up
+// (four ancestors per round trip); 0: level by level
+#ifndef SVG_PPUSH_SIFT
+#define SVG_PPUSH_SIFT 0
+#endif
 // 1: propagate() builds, tests and pushes one child window at a time through
-// one copy of the code (fewer live registers)
+// one copy of the code (fewer live registers; measured 10 % faster)
 #ifndef SVG_SEQ_CHILD
 #define SVG_SEQ_CHILD 1
 #endif
 // 1: the vertex ids of the top window's face are loaded before its pop's
 // sift-down, so propagate() issues its table probes with the face loads
+// (measured no faster: off)
 #ifndef SVG_FACE_IDS
-#define SVG_FACE_IDS 1
+#define SVG_FACE_IDS 0
 #endif
 
 namespace svgb {
@@ -336,6 +349,12 @@ struct LaneSmem {
     int32_t cross[128];
     int32_t windows[128], pseudos[128], generated[128], maxw[128], maxp[128];
     long long steps[128];
+    double twkey[128];  // heap tops (SVG_TOP_CACHE)
+    int32_t twpsrc[128];
+    uint32_t twsb[128];
+    double tpkey[128];
+    int32_t tpvert[128];
+    uint32_t tplb[128];
 };
 __shared__ LaneSmem g_lane_smem;
 #endif
@@ -365,6 +384,42 @@ struct LaneT {
     __device__ __forceinline__ VSlot* VT() const { return C.vtab + ((size_t)lid << C.vcap_log2); }
     __device__ __forceinline__ int32_t* VL() const { return C.vlist + (size_t)lid * C.vlimit; }
     __device__ __forceinline__ SSlot* ST() const { return C.stab + ((size_t)lid << C.scap_log2); }
+    // Heap tops (SVG_TOP_CACHE, one-thread form): equal to WH()[1] / PH()[1]
+    // whenever the heap is not empty.
+#if SVG_TOP_CACHE && SVG_SMEM_STATE
+    __device__ __forceinline__ void set_wtop(const WinEntry& e) const {
+        const int t = threadIdx.x;
+        g_lane_smem.twkey[t] = e.key; g_lane_smem.twpsrc[t] = e.psrc; g_lane_smem.twsb[t] = e.sb;
+    }
+    __device__ __forceinline__ void set_ptop(const PsEntry& e) const {
+        const int t = threadIdx.x;
+        g_lane_smem.tpkey[t] = e.key; g_lane_smem.tpvert[t] = e.vert; g_lane_smem.tplb[t] = e.lb;
+    }
+    __device__ __forceinline__ WinEntry wtop() const {
+        const int t = threadIdx.x;
+        WinEntry e;
+        e.key = g_lane_smem.twkey[t]; e.psrc = g_lane_smem.twpsrc[t]; e.sb = g_lane_smem.twsb[t];
+        return e;
+    }
+    __device__ __forceinline__ PsEntry ptop() const {
+        const int t = threadIdx.x;
+        PsEntry e;
+        e.key = g_lane_smem.tpkey[t]; e.vert = g_lane_smem.tpvert[t]; e.lb = g_lane_smem.tplb[t];
+        return e;
+    }
+#elif SVG_TOP_CACHE
+    WinEntry tw_;
+    PsEntry tp_;
+    __device__ __forceinline__ void set_wtop(const WinEntry& e) { tw_ = e; }
+    __device__ __forceinline__ void set_ptop(const PsEntry& e) { tp_ = e; }
+    __device__ __forceinline__ WinEntry wtop() const { return tw_; }
+    __device__ __forceinline__ PsEntry ptop() const { return tp_; }
+#else
+    __device__ __forceinline__ void set_wtop(const WinEntry&) const {}
+    __device__ __forceinline__ void set_ptop(const PsEntry&) const {}
+    __device__ __forceinline__ WinEntry wtop() const { return WH()[1]; }
+    __device__ __forceinline__ PsEntry ptop() const { return PH()[1]; }
+#endif
     int wsize, psize, nfree, nfresh;
     int ftop;       // WF()[nfree - 1] when nfree > 0 (free-slot cache)
     int vcount, scount;
@@ -601,7 +656,7 @@ struct LaneT {
     // no data-dependent branch splits the lanes; a higher climb continues level
     // by level.
     template <class T>
-    __device__ __forceinline__ void sift_up(T* H, int cur, const T& x) {
+    __device__ __forceinline__ int sift_up(T* H, int cur, const T& x) {
         if constexpr (kCoop) {
             // thread j holds ancestor cur >> (j + 1); the moves are the
             // ancestors, from the parent up, whose key exceeds x's
@@ -615,6 +670,7 @@ struct LaneT {
             if (lane < m) H[cur >> lane] = e;
             H[cur >> m] = x;
             __syncwarp();
+            return cur >> m;
         } else {
 #if SVG_KEYS_ONLY_SIFT
             // keys of the first four ancestors in one round trip; the moved
@@ -663,6 +719,7 @@ struct LaneT {
                 }
             }
             H[c] = x;
+            return c;
         }
     }
 
@@ -695,7 +752,8 @@ struct LaneT {
         e.key = w.key;
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        sift_up(WH(), ++wsize, e);
+        const int at = sift_up(WH(), ++wsize, e);
+        if (at == 1) set_wtop(e);
         if (wsize > st_maxw()) st_maxw() = wsize;
     }
     // Cooperative sift-down: the 62 nodes 1-5 levels below `cur` are loaded
@@ -751,7 +809,9 @@ struct LaneT {
     // again from the sectors just fetched and written with predicated stores,
     // one exit test per two levels.
     template <class T>
-    __device__ __forceinline__ int sift_down2(T* H, int n, const T& last) {
+    // nt receives the heap's new top entry (its root after the sift).
+    __device__ __forceinline__ int sift_down2(T* H, int n, const T& last, T& nt) {
+        nt = last;
         if constexpr (kCoop) return coop_sift_down(H, n, last);
         int cur = 1;
         for (;;) {
@@ -789,6 +849,7 @@ struct LaneT {
             if (mv1) e1 = H[c1];
             if (mv2) e2 = H[c2];
             if (mv3) e3 = H[c3];
+            if (l == 2 && mv1) nt = e1;
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             if (mv3) H[c2] = e3;
@@ -810,6 +871,7 @@ struct LaneT {
             T e1, e2;
             if (mv1) e1 = H[c1];
             if (mv2) e2 = H[c2];
+            if (l == 2 && mv1) nt = e1;
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             cur = mv2 ? c2 : (mv1 ? c1 : cur);
@@ -822,6 +884,7 @@ struct LaneT {
             const int k1 = (l + 1 <= n && !(a.key < b.key)) ? 1 : 0;
             const T e1 = k1 ? b : a;
             const bool mv1 = e1.key < last.key;
+            if (l == 2 && mv1) nt = e1;
             const int c1 = l + k1;
             const int l2 = c1 << 1;
             const T a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
@@ -838,11 +901,13 @@ struct LaneT {
         return cur;
     }
     __device__ WinEntry wpop() {
-        WinEntry top = WH()[1];
+        const WinEntry top = (SVG_TOP_CACHE && !kCoop) ? wtop() : WH()[1];
         WinEntry last = WH()[wsize];
         const int n = --wsize;
-        const int cur = sift_down2(WH(), n, last);
+        WinEntry nt;
+        const int cur = sift_down2(WH(), n, last, nt);
         WH()[cur] = last;
+        set_wtop(nt);
         WF()[nfree++] = (uint16_t)(top.sb & 0xFFFF);
         ftop = (int)(top.sb & 0xFFFF);
         if constexpr (kCoop) __syncwarp();
@@ -861,6 +926,9 @@ struct LaneT {
         e.key = key; e.vert = vert; e.lb = ((uint32_t)level << 8) | (uint32_t)(birth & 0xFF);
         if constexpr (kCoop) {
             sift_up(PH(), ++psize, e);
+        } else if (SVG_PPUSH_SIFT) {
+            const int at = sift_up(PH(), ++psize, e);
+            if (at == 1) set_ptop(e);
         } else {
             int cur = ++psize, p = cur >> 1;
             while (p > 0) {
@@ -871,15 +939,18 @@ struct LaneT {
                 p = cur >> 1;
             }
             ph(cur) = e;
+            if (cur == 1) set_ptop(e);
         }
         if (psize > st_maxp()) st_maxp() = psize;
     }
     __device__ PsEntry ppop() {
-        PsEntry top = PH()[1];
+        const PsEntry top = (SVG_TOP_CACHE && !kCoop) ? ptop() : PH()[1];
         PsEntry last = PH()[psize];
         const int n = --psize;
-        const int cur = sift_down2(PH(), n, last);
+        PsEntry nt;
+        const int cur = sift_down2(PH(), n, last, nt);
         PH()[cur] = last;
+        set_ptop(nt);
         if constexpr (kCoop) __syncwarp();
         return top;
     }
@@ -1426,8 +1497,13 @@ struct LaneT {
         PsEntry pp;
         pw.key = 0.0; pw.psrc = 0; pw.sb = 0;
         pp.key = 0.0; pp.vert = 0; pp.lb = 0;
-        if (wsize > 0) pw = WH()[1];
-        if (psize > 0) pp = PH()[1];
+        if (SVG_TOP_CACHE && !kCoop) {
+            if (wsize > 0) pw = wtop();
+            if (psize > 0) pp = ptop();
+        } else {
+            if (wsize > 0) pw = WH()[1];
+            if (psize > 0) pp = PH()[1];
+        }
         set_pk(pw, pp);
         // both birth lookups issued together
         const bool wlook = wsize > 0 && pw.psrc != source;
