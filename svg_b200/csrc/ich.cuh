@@ -85,6 +85,15 @@
 #ifndef SVG_PPUSH_SIFT
 #define SVG_PPUSH_SIFT 0
 #endif
+// 1: propagate() inserts a missing vertex or split entry at the empty slot its
+// lookup ended on (no second probe walk)
+#ifndef SVG_INSERT_AT
+#define SVG_INSERT_AT 1
+#endif
+// 1: propagate() prefetches into L1 the heap slots its pushes read first
+#ifndef SVG_PUSH_PREFETCH
+#define SVG_PUSH_PREFETCH 0
+#endif
 // 1: propagate() builds, tests and pushes one child window at a time through
 // one copy of the code (fewer live registers; measured 10 % faster)
 #ifndef SVG_SEQ_CHILD
@@ -531,7 +540,8 @@ struct LaneT {
         k = *reinterpret_cast<const int4*>(&VT()[h]);
         d = VT()[h].dist;
     }
-    __device__ __forceinline__ int vfinish(int v, uint32_t h, int4& k, double& d) const {
+    // h ends at the key's slot, or at the empty slot where an insert goes
+    __device__ __forceinline__ int vfinish(int v, uint32_t& h, int4& k, double& d) const {
         const uint32_t mask = (1u << C.vcap_log2) - 1;
         for (;;) {
             if ((uint32_t)k.y != epoch) { d = DBL_MAX; return -1; }
@@ -547,7 +557,7 @@ struct LaneT {
         dx = *reinterpret_cast<const double2*>(&ST()[h].dist);
     }
     // returns the slot or -1; dx = {dist, x} of the entry, {DBL_MAX, DBL_MAX} if absent
-    __device__ __forceinline__ int sfinish(int e, uint32_t h, int4& k, double2& dx) const {
+    __device__ __forceinline__ int sfinish(int e, uint32_t& h, int4& k, double2& dx) const {
         const uint32_t mask = (1u << C.scap_log2) - 1;
         for (;;) {
             if ((uint32_t)k.y != epoch) { dx.x = DBL_MAX; dx.y = DBL_MAX; return -1; }
@@ -582,6 +592,10 @@ struct LaneT {
                 h = (h + 1) & mask;
             }
         }
+        return vinsert(v, h);
+    }
+    // Insert vertex v at h, the empty slot that ends its probe chain.
+    __device__ int vinsert(int v, uint32_t h) {
         if (vcount >= C.vlimit) {  // keep the probe chains short: hand the source to the big pass
             flags |= kFlagCapacity;
             return -1;
@@ -620,6 +634,10 @@ struct LaneT {
                 h = (h + 1) & mask;
             }
         }
+        return sinsert(e, h);
+    }
+    // Insert half-edge e at h, the empty slot that ends its probe chain.
+    __device__ int sinsert(int e, uint32_t h) {
         if (scount >= C.slimit) {
             flags |= kFlagCapacity;
             return -1;
@@ -1116,6 +1134,20 @@ struct LaneT {
                 vfirst(B, hB, kB, dB);
                 vfirst(Cv, hC, kC, dC);
                 sfirst(e0, hS, kS, sdx);
+#if SVG_PUSH_PREFETCH
+                // the heap slots the children's sift-ups read first: the
+                // ancestors of positions wsize + 1 and wsize + 2, into L1
+                // while the probes are in flight
+                {
+                    const WinEntry* H = WH();
+                    const int p1 = wsize + 1, p2 = wsize + 2;
+#pragma unroll
+                    for (int j = 1; j <= 4; ++j) {
+                        if ((p1 >> j) > 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(H + (p1 >> j)));
+                    }
+                    if ((p2 >> 1) != (p1 >> 1)) asm volatile("prefetch.global.L1 [%0];" ::"l"(H + (p2 >> 1)));
+                }
+#endif
                 vfinish(A, hA, kA, dA);
                 vfinish(B, hB, kB, dB);
                 sC = vfinish(Cv, hC, kC, dC);
@@ -1160,7 +1192,12 @@ struct LaneT {
                     int ssl = sS;
                     bool ok = true;
                     if (D < sd) {
+#if SVG_INSERT_AT
+                        // the lookup's chain ended at the empty slot (hS)
+                        ssl = sS >= 0 ? sS : (kCoop ? sput(e0) : sinsert(e0, hS));
+#else
                         ssl = sS >= 0 ? sS : sput(e0);
+#endif
                         if (ssl < 0) {
                             ok = false;  // table full: the source goes to the retry pass
                         } else {
@@ -1171,7 +1208,11 @@ struct LaneT {
                     }
                     if (ok && D < dC) {
                         if (dC == DBL_MAX) ++total;
+#if SVG_INSERT_AT
+                        const int s = sC >= 0 ? sC : (kCoop ? vput(Cv) : vinsert(Cv, hC));
+#else
                         const int s = sC >= 0 ? sC : vput(Cv);
+#endif
                         if (s < 0) {
                             ok = false;
                         } else {
@@ -1529,8 +1570,12 @@ struct LaneT {
             // the top window's half-edge, loaded in the same round trip as the
             // birth probes (its sector is the payload's, read again when the
             // window is popped)
+#if SVG_FACE_IDS || SVG_FACE_PREFETCH
             const int cross = wsize > 0 ? WP()[pw.sb & 0xFFFF].cross : -1;
             set_pk_cross(cross);
+#else
+            const int cross = -1;
+#endif
             if (wlook) wb = vfinish(pw.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
             if (plook) pb = vfinish(pp.vert, hp, kp, dp) < 0 ? -1 : kp.w;
             if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
