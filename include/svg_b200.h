@@ -251,7 +251,7 @@ svg_status svg_msad_batch_device(svg_graph* g, int32_t n, const int64_t* d_set_o
  * to an outer framework's pool, or that runs where a cudaMalloc would
  * synchronise the device or break a capture.  The caller provides every
  * buffer; the kernel's scratch is a fixed array inside the library (about
- * 19 MiB per GPU that loads the library, held until the library unloads),
+ * 29 MiB per GPU that loads the library, held until the library unloads),
  * with tables sized as svg_build's first pass sizes them at K = 128.
  *   m            a mesh already on the device (svg_mesh_upload, which does
  *                allocate, must have been called earlier)

@@ -76,9 +76,10 @@
 #endif
 // 1: the lane keeps copies of its two heap tops, updated by every push and
 // pop (a pop's sift-down reads the new top anyway), so a look at the tops
-// costs no global round trip
+// needs no load.  Measured 5 % slower: the top's load hits L1 and the copies
+// cost registers (or shared-memory traffic).  Off.
 #ifndef SVG_TOP_CACHE
-#define SVG_TOP_CACHE 1
+#define SVG_TOP_CACHE 0
 #endif
 // 1: the one-thread pseudo-source push climbs with the window push's sift-up
 // (four ancestors per round trip); 0: level by level
