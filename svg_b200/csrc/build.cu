@@ -556,8 +556,8 @@ struct Layout {
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
-// heap entries per lane: the sift-down reads up to index cap + 7
-int heap_stride(int cap) { return (cap + 8 + 3) / 4 * 4; }
+// heap entries per lane: the sift-down reads up to index cap + 15
+int heap_stride(int cap) { return (cap + 16 + 3) / 4 * 4; }
 
 size_t lane_bytes(const Layout& l) {
     size_t b = 0;
@@ -1590,7 +1590,7 @@ constexpr int kStaticVlimit = (3 << kStaticVcapLog2) / 4;
 constexpr int kStaticSlimit = (3 << kStaticScapLog2) / 4;
 
 constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
-constexpr int kStaticStride = (kStaticWcap + 8 + 3) / 4 * 4;  // heap entries per lane
+constexpr int kStaticStride = (kStaticWcap + 16 + 3) / 4 * 4;  // heap entries per lane
 constexpr size_t kSzWheap = al256((size_t)kStaticLanes * kStaticStride * sizeof(WinEntry));
 constexpr size_t kSzWpool = al256((size_t)kStaticLanes * kStaticWcap * sizeof(WinPay));
 constexpr size_t kSzWfree = al256((size_t)kStaticLanes * kStaticWcap * sizeof(uint16_t));

@@ -53,6 +53,11 @@
 #ifndef SVG_KEYS_ONLY_SIFT
 #define SVG_KEYS_ONLY_SIFT 1
 #endif
+// 1: the one-thread sift-down reads the keys of four levels per round trip
+// (overrides SVG_SIFT3)
+#ifndef SVG_SIFT4
+#define SVG_SIFT4 0
+#endif
 // 1: the one-thread sift-down reads the keys of three levels per round trip
 // (measured 2.6 % faster on the 72.9K height field at K = 500, 4 % on the
 // 750K torus)
@@ -176,7 +181,7 @@ struct LaneConfig {
     int32_t wcap, pcap;      // logical queue capacities: pushes beyond them are dropped (reference)
     int32_t wphys, pphys;    // physical heap capacities (<= logical); exceeding one hands the
                              // source to the retry pass, which runs with physical = logical
-    int32_t wstride, pstride;// heap entries per lane (>= phys + 8, multiple of 4)
+    int32_t wstride, pstride;// heap entries per lane (>= phys + 16, multiple of 4)
     uint32_t vref, sref;     // the reference's table sizes, K*vert_coef and K*split_coef
     int32_t vcap_log2, scap_log2;
     int32_t vlimit, slimit;  // max keys this lane's tables take before kFlagCapacity
@@ -824,7 +829,7 @@ struct LaneT {
     // up while it is smaller than the last element.  The keys of the children
     // and grandchildren of `cur` are loaded together, so two levels cost one
     // dependent round trip (reads past the heap's end stay inside the lane's
-    // array, stride >= cap + 8, and are never used); the moved entries are read
+    // array, stride >= cap + 16, and are never used); the moved entries are read
     // again from the sectors just fetched and written with predicated stores,
     // one exit test per two levels.
     template <class T>
@@ -836,10 +841,75 @@ struct LaneT {
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
-#if SVG_SIFT3
+#if SVG_SIFT4
+            // keys of four levels below cur (2 + 4 + 8 + 16) in one round trip
+            // (reads past the heap's end stay inside the lane's array, stride
+            // >= cap + 16, and are never used); the moved entries are read
+            // again from the sectors just fetched
+            const double a = H[l].key, b = H[l + 1].key;
+            const int g = cur << 2, h8 = cur << 3, h16 = cur << 4;
+            double q[4], r[8], t[16];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) q[i] = 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) r[i] = 0.0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) t[i] = 0.0;
+            if (g <= n) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) q[i] = H[g + i].key;
+            }
+            if (h8 <= n) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) r[i] = H[h8 + i].key;
+            }
+            if (h16 <= n) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) t[i] = H[h16 + i].key;
+            }
+            const int k1 = (l + 1 <= n && !(a < b)) ? 1 : 0;
+            const bool mv1 = (k1 ? b : a) < last.key;
+            const int c1 = l + k1;
+            const int l2 = c1 << 1;
+            const double a2 = k1 ? q[2] : q[0], b2 = k1 ? q[3] : q[1];
+            const int k2 = (l2 + 1 <= n && !(a2 < b2)) ? 1 : 0;
+            const bool mv2 = mv1 && l2 <= n && (k2 ? b2 : a2) < last.key;
+            const int c2 = l2 + k2;
+            const int l3 = c2 << 1;  // = h8 + 4 k1 + 2 k2
+            const double a3 = k1 ? (k2 ? r[6] : r[4]) : (k2 ? r[2] : r[0]);
+            const double b3 = k1 ? (k2 ? r[7] : r[5]) : (k2 ? r[3] : r[1]);
+            const int k3 = (l3 + 1 <= n && !(a3 < b3)) ? 1 : 0;
+            const bool mv3 = mv2 && l3 <= n && (k3 ? b3 : a3) < last.key;
+            const int c3 = l3 + k3;
+            const int l4 = c3 << 1;  // = h16 + 8 k1 + 4 k2 + 2 k3
+            double ua[4], ub[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ua[i] = k1 ? t[8 + 2 * i] : t[2 * i];
+                ub[i] = k1 ? t[9 + 2 * i] : t[2 * i + 1];
+            }
+            const double va0 = k2 ? ua[2] : ua[0], va1 = k2 ? ua[3] : ua[1];
+            const double vb0 = k2 ? ub[2] : ub[0], vb1 = k2 ? ub[3] : ub[1];
+            const double a4 = k3 ? va1 : va0, b4 = k3 ? vb1 : vb0;
+            const int k4 = (l4 + 1 <= n && !(a4 < b4)) ? 1 : 0;
+            const bool mv4 = mv3 && l4 <= n && (k4 ? b4 : a4) < last.key;
+            const int c4 = l4 + k4;
+            T e1, e2, e3, e4;
+            if (mv1) e1 = H[c1];
+            if (mv2) e2 = H[c2];
+            if (mv3) e3 = H[c3];
+            if (mv4) e4 = H[c4];
+            if (l == 2 && mv1) nt = e1;
+            if (mv1) H[cur] = e1;
+            if (mv2) H[c1] = e2;
+            if (mv3) H[c2] = e3;
+            if (mv4) H[c3] = e4;
+            cur = mv4 ? c4 : (mv3 ? c3 : (mv2 ? c2 : (mv1 ? c1 : cur)));
+            const bool more = mv4;
+#elif SVG_SIFT3
             // keys of three levels below cur (2 + 4 + 8) in one round trip
             // (reads past the heap's end stay inside the lane's array,
-            // stride >= cap + 8, and are never used); the moved entries are
+            // stride >= cap + 16, and are never used); the moved entries are
             // read again from the sectors just fetched
             const double a = H[l].key, b = H[l + 1].key;
             const int g = cur << 2, h8 = cur << 3;
