@@ -41,10 +41,14 @@
 #ifndef SVG_SPLIT_SHIFT
 #define SVG_SPLIT_SHIFT SVG_TABLE_SHIFT
 #endif
+// threads per block the batched kernel is compiled for (the launch may use fewer)
+#ifndef SVG_ICH_TPB
+#define SVG_ICH_TPB 128
+#endif
 #if SVG_ICH_MIN_BLOCKS > 0
-#define SVG_ICH_BOUNDS __launch_bounds__(128, SVG_ICH_MIN_BLOCKS)
+#define SVG_ICH_BOUNDS __launch_bounds__(SVG_ICH_TPB, SVG_ICH_MIN_BLOCKS)
 #else
-#define SVG_ICH_BOUNDS __launch_bounds__(128)
+#define SVG_ICH_BOUNDS __launch_bounds__(SVG_ICH_TPB)
 #endif
 
 namespace svgb {
