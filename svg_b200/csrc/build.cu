@@ -41,6 +41,11 @@
 #ifndef SVG_SPLIT_SHIFT
 #define SVG_SPLIT_SHIFT SVG_TABLE_SHIFT
 #endif
+// 1: the path ends of the emitted rows are traced by a kernel of their own
+// (k_trace, one thread per edge) after k_emit
+#ifndef SVG_SPLIT_TRACE
+#define SVG_SPLIT_TRACE 1
+#endif
 // threads per block the batched kernel is compiled for (the launch may use fewer)
 #ifndef SVG_ICH_TPB
 #define SVG_ICH_TPB 128
@@ -452,6 +457,28 @@ struct EmitParams {
     int32_t smax;            // sort capacity per warp (power of two)
 };
 
+// Path ends of the emitted rows (k_emit with SVG_SPLIT_TRACE): one thread per
+// SVG edge whose path has a key point walks back from it to the source
+// (BuildGeodesicPathTo, ICHDevice.cu:336-480).  A walk is a chain of dependent
+// loads; run apart from the sort, with small blocks and few registers, many
+// more of them are in flight than inside k_emit's warps.
+__global__ void __launch_bounds__(256) k_trace(DevMesh M, PathEnd* path, int64_t nnz, int32_t* st_flags) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+        PathEnd pe = path[e];
+        if (!(pe.src_x < 0.0)) continue;
+        const int v = (int)pe.src_edge;
+        int fl = 0;
+        trace_direct(M, v, (int)pe.dst_edge, pe.dst_x, pe.src_edge, pe.src_x, fl);
+        if (pe.src_edge == 0xFFFFFFFFu) {
+            pe.src_edge = pe.dst_edge;
+            pe.src_x = pe.dst_x;
+        }
+        path[e] = pe;
+        if (fl) atomicOr(&st_flags[v], (fl & kFlagWatchdog) ? 4 : 8);
+    }
+}
+
 // Warp-per-source emission.
 __global__ void __launch_bounds__(256) k_emit(EmitParams P) {
     extern __shared__ unsigned long long sm_keys[];
@@ -507,11 +534,18 @@ __global__ void __launch_bounds__(256) k_emit(EmitParams P) {
                 } else {
                     pe.dst_edge = (uint32_t)c.ee;
                     pe.dst_x = c.x;
+#if SVG_SPLIT_TRACE
+                    // the path's first key point is traced by k_trace: the
+                    // source in src_edge, a negative src_x marks it pending
+                    pe.src_edge = (uint32_t)v;
+                    pe.src_x = -1.0;
+#else
                     trace_direct(P.M, v, c.ee, c.x, pe.src_edge, pe.src_x, fl);
                     if (pe.src_edge == 0xFFFFFFFFu) {
                         pe.src_edge = pe.dst_edge;
                         pe.src_x = pe.dst_x;
                     }
+#endif
                 }
                 P.path[base + i] = pe;
             }
@@ -562,6 +596,9 @@ size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 // heap entries per lane: the sift-down reads up to index cap + 15
 int heap_stride(int cap) { return (cap + 16 + 3) / 4 * 4; }
+
+// k_trace's grid: one thread per edge, at most 4,096 blocks of 256 (grid-stride)
+int trace_blocks(int64_t nnz) { return (int)std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, 4096)); }
 
 size_t lane_bytes(const Layout& l) {
     size_t b = 0;
@@ -788,7 +825,8 @@ bool replay_graph(svg_mesh* m, const svg_build_opts& o, svg_graph* g) {
     S.max_pseudo_queue = (int32_t)acc[4];
     S.edges = nnz;
     S.sources = bg->nsrc;
-    S.launches = 3;  // k_ich_batched, the offsets scan and k_emit, in one graph launch
+    S.launches = (SVG_SPLIT_TRACE && bg->opts.with_paths) ? 4 : 3;  // k_ich_batched, the offsets scan,
+                                                                     // k_emit (and k_trace), in one graph launch
     S.scratch_bytes = bg->scratch_bytes;
     S.coop_sources = bg->coop_n;
     S.coop_warps = bg->coop_warps;
@@ -901,6 +939,8 @@ void capture_graph(svg_mesh* m, const svg_build_opts& o, const CapturePlan& P, s
         SVG_CUDA(cub::DeviceScan::ExclusiveSum(bg->tmp.p, tb, d_deg, bg->off.as<int64_t>(), nv + 1, cs));
         SVG_CUDA(cudaEventRecordWithFlags(bg->ev[2], cs, cudaEventRecordExternal));
         k_emit<<<P.eb, P.wpb * 32, P.emit_smem, cs>>>(Em);
+        if (SVG_SPLIT_TRACE && P.with_paths && P.nnz > 0)
+            k_trace<<<trace_blocks(P.nnz), 256, 0, cs>>>(P.C.M, Em.path, P.nnz, Em.st_flags);
         SVG_CUDA(cudaEventRecordWithFlags(bg->ev[3], cs, cudaEventRecordExternal));
         SVG_CUDA(cudaStreamEndCapture(cs, &graph));
     } catch (...) {
@@ -1320,6 +1360,10 @@ svg_status run_build(svg_mesh* m, const svg_build_opts& o_in, svg_graph* g) {
         int eb = (int)std::min<int64_t>((nsrc + wpb - 1) / wpb, (int64_t)prop.multiProcessorCount * 16);
         k_emit<<<eb, wpb * 32, smem, st>>>(E);
         ++launches;
+        if (SVG_SPLIT_TRACE && g->with_paths && nnz > 0) {
+            k_trace<<<trace_blocks(nnz), 256, 0, st>>>(C.M, E.path, nnz, g->st_flags);
+            ++launches;
+        }
         cap_eb = eb;
         cap_wpb = wpb;
         cap_emit_smem = smem;
