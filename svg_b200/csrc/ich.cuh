@@ -53,6 +53,15 @@
 #ifndef SVG_KEYS_ONLY_SIFT
 #define SVG_KEYS_ONLY_SIFT 1
 #endif
+// keys-only sift-up: ancestors whose keys are read in one round trip
+#ifndef SVG_UP_LEVELS
+#define SVG_UP_LEVELS 4
+#endif
+// keys-only sift-up: up to this many ancestors, the moved entries are read
+// into registers together and then written; beyond it, one at a time
+#ifndef SVG_UP_ARRAY
+#define SVG_UP_ARRAY 4
+#endif
 // 1: the one-thread sift-down reads the keys of four levels per round trip
 // (overrides SVG_SIFT3)
 #ifndef SVG_SIFT4
@@ -698,24 +707,31 @@ struct LaneT {
             __syncwarp();
             return cur >> m;
         } else {
+            constexpr int kUp = SVG_KEYS_ONLY_SIFT ? SVG_UP_LEVELS : 4;
 #if SVG_KEYS_ONLY_SIFT
-            // keys of the first four ancestors in one round trip; the moved
+            // keys of the first kUp ancestors in one round trip; the moved
             // entries are read again (their sectors were just fetched) before
             // each is written one level down
-            double ak[4];
+            double ak[kUp];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ak[j] = (cur >> (j + 1)) > 0 ? H[cur >> (j + 1)].key : 0.0;
+            for (int j = 0; j < kUp; ++j) ak[j] = (cur >> (j + 1)) > 0 ? H[cur >> (j + 1)].key : 0.0;
             int m = 0;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < kUp; ++j)
                 if (m == j && (cur >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
-            T mv[4];
+            if constexpr (kUp <= SVG_UP_ARRAY) {
+                T mv[kUp];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (j < m) mv[j] = H[cur >> (j + 1)];
+                for (int j = 0; j < kUp; ++j)
+                    if (j < m) mv[j] = H[cur >> (j + 1)];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (j < m) H[cur >> j] = mv[j];
+                for (int j = 0; j < kUp; ++j)
+                    if (j < m) H[cur >> j] = mv[j];
+            } else {
+                // one entry at a time, top-down reads after the writes below
+                // them (each read hits the sector just fetched)
+                for (int j = 0; j < m; ++j) H[cur >> j] = H[cur >> (j + 1)];
+            }
 #else
             // the first four ancestors in one round trip (they are what the level-
             // by-level loop would read: a move only writes below the next
@@ -734,7 +750,7 @@ struct LaneT {
                 if (j < m) H[cur >> j] = anc[j];
 #endif
             int c = cur >> m;
-            if (m == 4) {
+            if (m == kUp) {
                 for (;;) {
                     const int p = c >> 1;
                     if (p == 0) break;
