@@ -78,15 +78,6 @@ svg_status svg_mesh_counts(const svg_mesh* m, int32_t* nv, int32_t* nf, int32_t*
 svg_status svg_mesh_export(const svg_mesh* m, int32_t* he_v0, int32_t* he_twin, double* he_len,
                            double* pos, double* angle, int32_t* first_edge);
 
-/* Host copies of the vertex fans the pseudo-source steps walk (any pointer may
- * be NULL): fan_edge[ne] holds, vertex by vertex, the outgoing half-edges of
- * each manifold vertex in the order o_{k+1} = next(twin(o_k)); ring_base[nv]
- * and ring_len2[nv] (2 * count + 1 if the fan is closed, 0 for a vertex with
- * no fan, whose half-edges are walked one by one); fan_pos[ne] = the index of
- * half-edge e in fan_edge, -1 if its vertex has no fan. */
-svg_status svg_mesh_export_fans(const svg_mesh* m, int32_t* fan_edge, int32_t* fan_pos, int32_t* ring_base,
-                                int32_t* ring_len2);
-
 /* ------------------------------------------------------------------ build */
 
 typedef enum svg_build_mode {

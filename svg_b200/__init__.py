@@ -113,7 +113,6 @@ EXPORTS = [
     "svg_server_poll", "svg_server_take", "svg_server_stats", "svg_server_submit_msad_into",
     "svg_device_memory", "svg_graph_set_query_form", "svg_server_resident",
     "svg_msad_batch_paths", "svg_sssd_path", "svg_device_fp64_rate", "svg_build_autotune",
-    "svg_mesh_export_fans",
 ]
 
 _lib = None
@@ -136,7 +135,6 @@ def lib() -> C.CDLL:
     L.svg_mesh_free.restype = None
     L.svg_mesh_counts.argtypes = [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.svg_mesh_export.argtypes = [_P] + [_P] * 6
-    L.svg_mesh_export_fans.argtypes = [_P] + [_P] * 4
     L.svg_build_opts_default.argtypes = [C.POINTER(BuildOptions)]
     L.svg_build_opts_default.restype = None
     L.svg_build.argtypes = [_P, C.POINTER(BuildOptions), C.POINTER(_P)]
@@ -233,15 +231,6 @@ class Mesh:
                    pos=np.zeros((V, 3)), angle=np.zeros(V), first_edge=np.zeros(V, np.int32))
         _check(lib().svg_mesh_export(self._h, *[out[k].ctypes.data_as(_P) for k in
                                                 ["he_v0", "he_twin", "he_len", "pos", "angle", "first_edge"]]))
-        return out
-
-    def export_fans(self) -> dict:
-        """svg_mesh_export_fans: the vertex fans the pseudo-source steps walk."""
-        V, E = self.vertNum, self.edgeNum
-        out = dict(fan_edge=np.zeros(E, np.int32), fan_pos=np.zeros(E, np.int32),
-                   ring_base=np.zeros(V, np.int32), ring_len2=np.zeros(V, np.int32))
-        _check(lib().svg_mesh_export_fans(self._h, *[out[k].ctypes.data_as(_P) for k in
-                                                     ["fan_edge", "fan_pos", "ring_base", "ring_len2"]]))
         return out
 
 

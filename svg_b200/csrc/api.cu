@@ -144,9 +144,6 @@ DevMesh MeshDev::view() const {
     v.geo = geo;
     v.vr = vr;
     v.pos = pos;
-    v.fan = fan;
-    v.fanpos = fanpos;
-    v.ring = ring;
     return v;
 }
 
@@ -159,34 +156,18 @@ void upload_mesh(svg_mesh* m) {
     // one block, half-edge records first: the records a window step reads
     // form one contiguous range (an L2 access-policy window can cover it)
     const size_t b_he = al256(sizeof(HeRec) * (size_t)H.ne), b_geo = al256(sizeof(HeGeo) * (size_t)H.ne),
-                 b_vr = al256(sizeof(VertRec) * (size_t)H.nv), b_pos = al256(sizeof(double) * 3 * (size_t)H.nv),
-                 b_fan = al256(sizeof(FanRec) * (size_t)H.ne), b_fanpos = al256(sizeof(int32_t) * (size_t)H.ne),
-                 b_ring = al256(sizeof(RingRec) * (size_t)H.nv);
-    const size_t total = b_he + b_geo + b_vr + b_pos + b_fan + b_fanpos + b_ring;
-    char* blk = static_cast<char*>(dev_alloc(total));
+                 b_vr = al256(sizeof(VertRec) * (size_t)H.nv), b_pos = al256(sizeof(double) * 3 * (size_t)H.nv);
+    char* blk = static_cast<char*>(dev_alloc(b_he + b_geo + b_vr + b_pos));
     D.block = blk;
-    D.block_bytes = total;
-    size_t at = 0;
-    D.he = reinterpret_cast<HeRec*>(blk + at);
-    at += b_he;
-    D.geo = reinterpret_cast<HeGeo*>(blk + at);
-    at += b_geo;
-    D.vr = reinterpret_cast<VertRec*>(blk + at);
-    at += b_vr;
-    D.pos = reinterpret_cast<double*>(blk + at);
-    at += b_pos;
-    D.fan = reinterpret_cast<FanRec*>(blk + at);
-    at += b_fan;
-    D.fanpos = reinterpret_cast<int32_t*>(blk + at);
-    at += b_fanpos;
-    D.ring = reinterpret_cast<RingRec*>(blk + at);
+    D.block_bytes = b_he + b_geo + b_vr + b_pos;
+    D.he = reinterpret_cast<HeRec*>(blk);
+    D.geo = reinterpret_cast<HeGeo*>(blk + b_he);
+    D.vr = reinterpret_cast<VertRec*>(blk + b_he + b_geo);
+    D.pos = reinterpret_cast<double*>(blk + b_he + b_geo + b_vr);
     SVG_CUDA(cudaMemcpyAsync(D.he, H.he.data(), sizeof(HeRec) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.geo, H.geo.data(), sizeof(HeGeo) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.vr, H.vr.data(), sizeof(VertRec) * (size_t)H.nv, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaMemcpyAsync(D.pos, H.pos.data(), sizeof(double) * 3 * (size_t)H.nv, cudaMemcpyHostToDevice, st));
-    SVG_CUDA(cudaMemcpyAsync(D.fan, H.fan.data(), sizeof(FanRec) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
-    SVG_CUDA(cudaMemcpyAsync(D.fanpos, H.fanpos.data(), sizeof(int32_t) * (size_t)H.ne, cudaMemcpyHostToDevice, st));
-    SVG_CUDA(cudaMemcpyAsync(D.ring, H.ring.data(), sizeof(RingRec) * (size_t)H.nv, cudaMemcpyHostToDevice, st));
     SVG_CUDA(cudaStreamSynchronize(st));
     D.nv = H.nv;
     D.nf = H.nf;
@@ -333,24 +314,6 @@ svg_status svg_mesh_export(const svg_mesh* m, int32_t* he_v0, int32_t* he_twin, 
     if (pos) std::memcpy(pos, H.pos.data(), sizeof(double) * 3 * (size_t)H.nv);
     if (angle) std::memcpy(angle, H.angle.data(), sizeof(double) * (size_t)H.nv);
     for (int32_t v = 0; v < H.nv && first_edge; ++v) first_edge[v] = H.vr[v].first;
-    return SVG_OK;
-}
-
-svg_status svg_mesh_export_fans(const svg_mesh* m, int32_t* fan_edge, int32_t* fan_pos, int32_t* ring_base,
-                                int32_t* ring_len2) {
-    if (!m) {
-        set_error("null mesh");
-        return SVG_ERR_ARG;
-    }
-    const HostMesh& H = m->h;
-    for (int32_t e = 0; e < H.ne; ++e) {
-        if (fan_edge) fan_edge[e] = H.fan[e].o;
-        if (fan_pos) fan_pos[e] = H.fanpos[e];
-    }
-    for (int32_t v = 0; v < H.nv; ++v) {
-        if (ring_base) ring_base[v] = H.ring[v].base;
-        if (ring_len2) ring_len2[v] = H.ring[v].len2;
-    }
     return SVG_OK;
 }
 

@@ -59,16 +59,13 @@ struct DevBuf {
 
 struct MeshDev {
     bool uploaded = false;
-    void* block = nullptr;   // one allocation holding he, geo, vr, pos, fan, fanpos, ring in that order
+    void* block = nullptr;   // one allocation holding he, geo, vr, pos in that order
     size_t block_bytes = 0;
     int32_t nv = 0, nf = 0, ne = 0;
     HeRec* he = nullptr;
     HeGeo* geo = nullptr;
     VertRec* vr = nullptr;
     double* pos = nullptr;
-    FanRec* fan = nullptr;
-    int32_t* fanpos = nullptr;
-    RingRec* ring = nullptr;
     DevMesh view() const;
 };
 

@@ -106,11 +106,6 @@
 #ifndef SVG_INSERT_AT
 #define SVG_INSERT_AT 1
 #endif
-// 1: a pseudo-source step on a vertex with a fan (FanRec) walks the fan's
-// records instead of chasing half-edge twins (one-thread form)
-#ifndef SVG_FANS
-#define SVG_FANS 1
-#endif
 // 1: propagate() prefetches into L1 the heap slots its pushes read first
 // (measured no faster: off)
 #ifndef SVG_PUSH_PREFETCH
@@ -1398,94 +1393,19 @@ struct LaneT {
         if (cur != -1) endEdge = ld_he(M.he, nxt(nxt(ld_he(M.he, cur).twin))).twin;
     }
 
-    // A vertex's fan (FanRec) in fan indices: n records from fb, o_{k+1} =
-    // next(twin(o_k)) (step_b) and o_{k-1} = twin(prev(o_k)) (step_f),
-    // wrapping on a closed fan and -1 past an open one's ends.
-    struct FanIx {
-        int fb, n;
-        bool closed;
-    };
-    __device__ __forceinline__ static int step_b(const FanIx& f, int k) {
-        return k + 1 < f.n ? k + 1 : (f.closed ? 0 : -1);
-    }
-    __device__ __forceinline__ static int step_f(const FanIx& f, int k) {
-        return k > 0 ? k - 1 : (f.closed ? f.n - 1 : -1);
-    }
-    // fan index of half-edge e leaving the fan's vertex (-1 if not on the fan)
-    __device__ __forceinline__ int fan_index(const FanIx& f, int e) const {
-        const int p = __ldg(&C.M.fanpos[e]) - f.fb;
-        return (p >= 0 && p < f.n) ? p : -1;
-    }
-    // fan_walk over fan indices: the first walk from index kl (-1: left is
-    // -1), the second from the half-edge after index kx (kx: the fan index of
-    // twin(right); its step_b is -1 when right is -1).  Same iterations, sums
-    // and guard as fan_walk; ks / ke are the fan indices of startEdge /
-    // endEdge.  Where fan_walk would take next() of a -1 twin (the reference
-    // reads edges[-1] there) it returns false: the caller walks the half-edges.
-    __device__ bool fan_walk_ix(const FanIx& f, int kl, int kx, double a0, double a1, int& ks, int& ke) {
-        const FanRec* R = C.M.fan + f.fb;
-        ks = -1;
-        ke = -1;
-        int k = kl, guard = 0;
-        while (a0 < kRefPi && k != -1) {
-            a0 += __ldg(&R[k].corner);
-            k = step_f(f, k);
-            if (++guard > 1 << 20) { flags |= kFlagWatchdog; return true; }
-        }
-        if (k != -1) {
-            ks = step_b(f, k);
-            if (ks < 0) return false;
-        }
-        int j = step_b(f, kx), jl = kx;
-        bool cur = j != -1;
-        while (a1 < kRefPi && cur) {
-            a1 += __ldg(&R[j].corner);
-            jl = j;
-            j = step_b(f, j);
-            cur = j != -1;
-            if (++guard > 1 << 20) { flags |= kFlagWatchdog; ks = -1; return true; }
-        }
-        if (cur) ke = step_f(f, jl);
-        return true;
-    }
-
     // ICHDevice::GenSubWinsForPseudoSrc (ICHDevice.cu:728-793).  Called by
-    // the lanes of `amask` together (see propagate); `live` predicates.  On a
-    // vertex with a fan (one-thread form) the walks read the fan's records.
+    // the lanes of `amask` together (see propagate); `live` predicates.
     __device__ void gen_sub_wins(double pdist, int pv, int plevel, int pbirth, bool live, unsigned amask) {
         const DevMesh& M = C.M;
         int startEdge = -1, endEdge = -1;
-#if SVG_FANS
-        int fks = -1, fke = -1, kfirst = 0;
-        bool fan = false;
-        FanIx fx{0, 0, false};
-#endif
         if (live) {
             int vs = vfind(pv);
-#if SVG_FANS
-            if constexpr (!kCoop) {
-                const int4 rr = __ldg(reinterpret_cast<const int4*>(M.ring + pv));
-                fx.fb = rr.x;
-                fx.n = rr.y >> 1;
-                fx.closed = (rr.y & 1) != 0;
-                kfirst = rr.z;
-                fan = fx.n > 0;
-            }
-#endif
             int enter = vs < 0 ? -1 : VT()[vs].enter;
             int vb = vs < 0 ? -1 : VT()[vs].birth;
             if (enter == -1 && vb != -1) {
                 startEdge = __ldg(&M.vr[pv].first);
                 endEdge = startEdge;
-#if SVG_FANS
-                fks = fke = kfirst;
-#endif
             } else if (enter >= 0 && ld_he(M.he, enter).v0 == pv) {
-#if SVG_FANS
-                const int ki = fan ? fan_index(fx, enter) : -1;
-                fan = ki >= 0 && fan_walk_ix(fx, ki, ki, 0.0, 0.0, fks, fke);
-                if (!fan)
-#endif
                 fan_walk(enter, ld_he(M.he, enter).twin, 0.0, 0.0, startEdge, endEdge);
             } else if (enter >= 0 && ld_he(M.he, nxt(enter)).v1 == pv) {
                 // GenSubWinsForPseudoSrcFromWindow (ICHDevice.cu:795-858)
@@ -1504,12 +1424,6 @@ struct LaneT {
                 if (a1 > 1.0) a1 = 1.0; else if (a1 < -1.0) a1 = -1.0;
                 a0 = acos(a0);
                 a1 = acos(a1);
-#if SVG_FANS
-                // left = twin(e1) = twin(prev(e2)): one step_f from e2; twin(right) = e2
-                const int k2 = fan ? fan_index(fx, e2) : -1;
-                fan = k2 >= 0 && fan_walk_ix(fx, step_f(fx, k2), k2, a0, a1, fks, fke);
-                if (!fan)
-#endif
                 fan_walk(h1.twin, h2.twin, a0, a1, startEdge, endEdge);
             } else {
                 flags |= kFlagUndefined;  // assert(false) at ICHDevice.cu:740
@@ -1518,30 +1432,6 @@ struct LaneT {
             if (flags & kFlagWatchdog) live = false;
         }
         __syncwarp(amask);
-#if SVG_FANS
-        if (live && fan) {
-            // the window loop over the fan: startEdge -> twin(prev(startEdge))
-            const FanRec* R = M.fan + fx.fb;
-            int guard = 0, k = fks;
-            do {
-                if (k < 0) {  // the reference reads edges[-1] here
-                    flags |= kFlagUndefined;
-                    break;
-                }
-                const double len = __ldg(&R[k].len), lnx = __ldg(&R[k].lnx), lpv = __ldg(&R[k].lpv);
-                const int tn = __ldg(&R[k].tn);
-                NewWin w;
-                finish_window(0.0, lnx, len, lpv, pdist, w);
-                w.p.cross = tn;
-                w.p.level = plevel + 1;
-                wpush(w, pv, pbirth);
-                k = step_f(fx, k);
-                if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
-            } while (k != fke);
-        }
-        if (!fan)
-#endif
-        {
 #if SVG_FAN_PIPE
         // The same walk with the next face's records loaded before this
         // face's push, so the two round trips overlap.
@@ -1595,40 +1485,8 @@ struct LaneT {
             } while (startEdge != endEdge);
         }
 #endif
-        }
         __syncwarp(amask);
-#if SVG_FANS
-        if (live && fan) {
-            // the neighbour loop over the fan from firstEdge: o -> next(twin(o))
-            const FanRec* R = M.fan + fx.fb;
-            int k = kfirst, guard = 0;
-            do {
-                if (++guard > 1 << 20) { flags |= kFlagWatchdog; break; }
-                const int kb = step_b(fx, k);
-                const int opv = __ldg(&R[k].v1);
-                const double hlen = __ldg(&R[k].len);
-                int os = vfind(opv);
-                double od = os < 0 ? DBL_MAX : VT()[os].dist;
-                if (!(__ldg(&M.vr[opv].flags) & kVertSaddleGE) || od < pdist + hlen) {
-                    k = kb;
-                    continue;
-                }
-                if (od == DBL_MAX) ++total;
-                int s = os < 0 ? vput(opv) : os;
-                if (s < 0) break;
-                VT()[s].dist = pdist + hlen;
-                int b = (int)(signed char)(VT()[s].birth + 1);
-                set_birth(s, opv, b);
-                VT()[s].enter = __ldg(&R[k].tw);
-                VT()[s].sslot = -1;
-                ppush(VT()[s].dist, opv, plevel, b);
-                k = kb;
-            } while (k != kfirst && k != -1);
-        }
-        if (!fan && live) {
-#else
         if (live) {
-#endif
             int start = __ldg(&M.vr[pv].first), cur = start;
             int guard = 0;
 #if SVG_FAN_PIPE

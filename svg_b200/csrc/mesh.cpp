@@ -99,78 +99,6 @@ void parallel_for(int64_t n, F fn) {
 }
 }  // namespace
 
-// Fans (FanRec): for each vertex, starting at its firstEdge, walk back with
-// twin(prev(.)) to the fan's start (the boundary, or around to firstEdge),
-// then forward with next(twin(.)), checking at each step that the two steps
-// are inverse, that the half-edge leaves the vertex, and at the end that every
-// outgoing half-edge was met once and the far vertices are distinct.  A vertex
-// that fails any check keeps no fan: the kernels walk its half-edges.
-static void build_fans(HostMesh& m) {
-    const int32_t nv = m.nv, E = m.ne;
-    auto nxt = [](int32_t e) { return e - e % 3 + (e % 3 + 1) % 3; };
-    auto prv = [](int32_t e) { return e - e % 3 + (e % 3 + 2) % 3; };
-    auto F = [&](int32_t o) { return m.he[prv(o)].twin; };
-    auto B = [&](int32_t o) { const int32_t t = m.he[o].twin; return t < 0 ? -1 : nxt(t); };
-    std::vector<int32_t> deg((size_t)nv + 1, 0);
-    for (int32_t e = 0; e < E; ++e) ++deg[(size_t)m.he[e].v0 + 1];
-    std::vector<int32_t> base((size_t)nv + 1, 0);
-    for (int32_t v = 0; v < nv; ++v) base[v + 1] = base[v] + deg[v + 1];
-    m.fan.assign((size_t)E, FanRec{});
-    m.fanpos.assign((size_t)E, -1);
-    m.ring.assign((size_t)nv, RingRec{0, 0, 0, 0});
-    parallel_for(nv, [&](int64_t b, int64_t v_end) {
-        std::vector<int32_t> seq, far;
-        for (int64_t vv = b; vv < v_end; ++vv) {
-            const int32_t v = (int32_t)vv, d = deg[(size_t)v + 1], s = m.vr[v].first;
-            m.ring[v] = RingRec{base[v], 0, 0, 0};
-            if (d == 0 || s < 0) continue;
-            // back to the start of the fan
-            int32_t a = s, steps = 0;
-            bool closed = false, ok = true;
-            for (;;) {
-                const int32_t p = F(a);
-                if (p < 0) break;
-                if (p == s) { closed = true; break; }
-                if (m.he[p].v0 != v || ++steps > d) { ok = false; break; }
-                a = p;
-            }
-            if (!ok) continue;
-            const int32_t start = closed ? s : a;
-            seq.clear();
-            int32_t cur = start;
-            for (;;) {
-                seq.push_back(cur);
-                if ((int32_t)seq.size() > d) { ok = false; break; }
-                const int32_t nb = B(cur);
-                if (nb < 0) { ok = !closed; break; }
-                if (nb == start) { ok = closed && F(start) == cur; break; }
-                if (m.he[nb].v0 != v || F(nb) != cur) { ok = false; break; }
-                cur = nb;
-            }
-            if (!ok || (int32_t)seq.size() != d) continue;
-            if (!closed && F(start) != -1) continue;
-            far.clear();
-            for (int32_t o : seq) far.push_back(m.he[o].v1);
-            std::sort(far.begin(), far.end());
-            if (std::adjacent_find(far.begin(), far.end()) != far.end()) continue;
-            for (int32_t k = 0; k < d; ++k) {
-                const int32_t o = seq[k];
-                FanRec& r = m.fan[(size_t)base[v] + k];
-                r.o = o;
-                r.v1 = m.he[o].v1;
-                r.tn = m.he[nxt(o)].twin;
-                r.tw = m.he[o].twin;
-                r.corner = m.he[o].corner;
-                r.len = m.he[o].len;
-                r.lnx = m.he[nxt(o)].len;
-                r.lpv = m.he[prv(o)].len;
-                m.fanpos[o] = base[v] + k;
-            }
-            m.ring[v] = RingRec{base[v], 2 * d + (closed ? 1 : 0), m.fanpos[s] - base[v], 0};
-        }
-    });
-}
-
 // Mesh::LoadFromFile (Mesh.cu:62-123) from arrays, plus the per-half-edge
 // geometry the kernels read instead of recomputing it per window.
 //
@@ -288,7 +216,6 @@ std::string build_host_mesh(int32_t nv, const double* pos, int32_t nf, const int
         if (m.angle[v] > 2.0 * kPi) fl |= kVertSaddleGT;     // saddle test of PropagateWindow
         m.vr[v].flags = fl;
     }
-    build_fans(m);
     return std::string();
 }
 

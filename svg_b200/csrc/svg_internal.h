@@ -38,40 +38,12 @@ struct VertRec {
     int32_t flags;
 };
 
-// The fan of a vertex v: its outgoing half-edges o_0, o_1, ... in the order
-// o_{k+1} = next(twin(o_k)) (the order the reference's walk over a vertex's
-// neighbours takes, ICHDevice.cu:775-790); twin(prev(o_{k+1})) = o_k.  Built
-// only where those two steps are inverse, every outgoing half-edge is on the
-// fan once and the neighbours are distinct (a manifold vertex, interior or on
-// one boundary); a closed fan wraps, an open one ends where a twin is -1.  One
-// record holds what a pseudo-source step reads per face of the fan, so a walk
-// over the fan reads consecutive records instead of chasing twins.
-struct alignas(16) FanRec {
-    int32_t o;       // the half-edge
-    int32_t v1;      // its far vertex
-    int32_t tn;      // twin(next(o)): the edge opposite v in face(o), seen from the next face
-    int32_t tw;      // twin(o)
-    double corner;   // corner(o): the angle at v in face(o)
-    double len;      // len(o)
-    double lnx;      // len(next(o))
-    double lpv;      // len(prev(o))
-};
-struct alignas(16) RingRec {
-    int32_t base;    // first record of the vertex's fan in the fan array
-    int32_t len2;    // 2 * records + (1 if the fan is closed); 0: no fan (walk the half-edges)
-    int32_t kfirst;  // fan index of the vertex's firstEdge
-    int32_t pad;
-};
-
 struct DevMesh {
     int32_t nv, nf, ne;
     const HeRec* he;
     const HeGeo* geo;
     const VertRec* vr;
     const double* pos;
-    const FanRec* fan;      // fans of the manifold vertices, by vertex
-    const int32_t* fanpos;  // half-edge -> its record in fan (-1: its vertex has no fan)
-    const RingRec* ring;    // vertex -> its fan
 };
 
 // Host half-edge construction (Mesh::LoadFromFile semantics).
@@ -105,9 +77,6 @@ struct HostMesh {
     std::vector<HeGeo, UninitAlloc<HeGeo>> geo;
     std::vector<VertRec> vr;
     std::vector<double> angle;
-    std::vector<FanRec> fan;
-    std::vector<int32_t> fanpos;
-    std::vector<RingRec> ring;
 };
 
 // Returns an empty string on success, else the reason.

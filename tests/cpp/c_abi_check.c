@@ -11,7 +11,6 @@ int main(void) {
     void* fns[] = {
         (void*)svg_last_error, (void*)svg_version, (void*)svg_mesh_load_obj, (void*)svg_mesh_from_arrays,
         (void*)svg_mesh_upload, (void*)svg_mesh_free, (void*)svg_mesh_counts, (void*)svg_mesh_export,
-        (void*)svg_mesh_export_fans,
         (void*)svg_build_opts_default, (void*)svg_build, (void*)svg_build_autotune, (void*)svg_graph_stats, (void*)svg_graph_source_stats,
         (void*)svg_graph_free, (void*)svg_graph_set_query_form, (void*)svg_graph_counts, (void*)svg_graph_copy_csr,
         (void*)svg_graph_copy_nodes, (void*)svg_graph_device_csr, (void*)svg_graph_save, (void*)svg_graph_load,

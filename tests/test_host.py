@@ -158,107 +158,3 @@ def test_random_meshes_match_reference_loader(seed):
         b = RefOracle().load(p, fix_boundary=True).export()
     for k in ["he_v0", "he_twin", "he_len", "angle", "first_edge"]:
         assert np.array_equal(a[k], b[k]), k
-
-
-def _fan_reference(he_v0, twin, first, nv):
-    """Which vertices get a fan and its half-edges, restated from the
-    half-edge steps the pseudo-source walks take: B(o) = next(twin(o)) around
-    a vertex, F(o) = twin(prev(o)) its inverse."""
-    E = len(he_v0)
-    nxt = lambda e: e - e % 3 + (e % 3 + 1) % 3
-    prv = lambda e: e - e % 3 + (e % 3 + 2) % 3
-    F = lambda o: int(twin[prv(o)])
-    B = lambda o: -1 if twin[o] < 0 else nxt(int(twin[o]))
-    deg = np.bincount(he_v0, minlength=nv)
-    fans = {}
-    for v in range(nv):
-        s = int(first[v])
-        if deg[v] == 0 or s < 0:
-            continue
-        a, closed, ok, steps = s, False, True, 0
-        while True:
-            p = F(a)
-            if p < 0:
-                break
-            if p == s:
-                closed = True
-                break
-            steps += 1
-            if he_v0[p] != v or steps > deg[v]:
-                ok = False
-                break
-            a = p
-        if not ok:
-            continue
-        start = s if closed else a
-        seq, cur = [], start
-        while True:
-            seq.append(cur)
-            if len(seq) > deg[v]:
-                ok = False
-                break
-            nb = B(cur)
-            if nb < 0:
-                ok = not closed
-                break
-            if nb == start:
-                ok = closed and F(start) == cur
-                break
-            if he_v0[nb] != v or F(nb) != cur:
-                ok = False
-                break
-            cur = nb
-        if not ok or len(seq) != deg[v]:
-            continue
-        far = [int(he_v0[nxt(o)]) for o in seq]
-        if len(set(far)) != len(far):
-            continue
-        fans[v] = (seq, closed)
-    return fans
-
-
-def _fan_cases():
-    yield "torus", meshgen.torus(1.0, 0.35, 20, 14, 0.02, seed=5)
-    yield "height_field", meshgen.height_field(24, 6, 0.2, seed=3)
-    # two triangles sharing only a vertex (a bowtie: the shared vertex has two fans)
-    yield "bowtie", (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [-1, 0, 0], [0, -1, 0]], float),
-                     np.array([[0, 1, 2], [0, 3, 4]], np.int32))
-    # three triangles on one edge (non-manifold) plus a closed fan elsewhere
-    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [2, 0, 0]], float)
-    faces = np.array([[0, 1, 2], [1, 0, 3], [0, 1, 4], [1, 5, 2]], np.int32)
-    yield "non_manifold", (pos, faces)
-
-
-@pytest.mark.parametrize("case", ["torus", "height_field", "bowtie", "non_manifold"])
-def test_vertex_fans_follow_the_half_edge_walks(case):
-    """The fans the pseudo-source steps read are exactly the half-edge walks
-    they replace, and only the vertices where those walks are well formed get
-    one (the kernels walk the half-edges of every other vertex)."""
-    build_lib()
-    pos, faces = dict(_fan_cases())[case]
-    m = Mesh.from_arrays(pos, faces)
-    ex = m.export()
-    fa = m.export_fans()
-    nv = len(pos)
-    fans = _fan_reference(ex["he_v0"], ex["he_twin"], ex["first_edge"], nv)
-    for v in range(nv):
-        L2 = int(fa["ring_len2"][v])
-        if v not in fans:
-            assert L2 == 0, f"vertex {v} got a fan"
-            continue
-        seq, closed = fans[v]
-        assert L2 == 2 * len(seq) + (1 if closed else 0)
-        b = int(fa["ring_base"][v])
-        assert list(fa["fan_edge"][b:b + len(seq)]) == seq
-        for k, o in enumerate(seq):
-            assert fa["fan_pos"][o] == b + k
-    has = np.zeros(len(ex["he_v0"]), bool)
-    for v, (seq, _) in fans.items():
-        has[seq] = True
-    assert np.all(fa["fan_pos"][~has] == -1)
-    if case in ("torus", "height_field"):
-        assert len(fans) == nv          # every vertex of a manifold mesh has a fan
-    if case == "bowtie":
-        assert 0 not in fans and len(fans) == 4
-    if case == "non_manifold":
-        assert 0 not in fans and 1 not in fans
