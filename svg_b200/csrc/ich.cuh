@@ -57,6 +57,11 @@
 #ifndef SVG_UP_LEVELS
 #define SVG_UP_LEVELS 4
 #endif
+// 1: the keys-only sift-up reads a further batch of ancestors' keys per round
+// trip while the climb goes on (0: one level per round trip past the first batch)
+#ifndef SVG_UP_BATCHES
+#define SVG_UP_BATCHES 1
+#endif
 // keys-only sift-up: up to this many ancestors, the moved entries are read
 // into registers together and then written; beyond it, one at a time
 #ifndef SVG_UP_ARRAY
@@ -708,7 +713,37 @@ struct LaneT {
             return cur >> m;
         } else {
             constexpr int kUp = SVG_KEYS_ONLY_SIFT ? SVG_UP_LEVELS : 4;
-#if SVG_KEYS_ONLY_SIFT
+#if SVG_KEYS_ONLY_SIFT && SVG_UP_BATCHES
+            // batches of kUp ancestors' keys, one round trip each, for as long
+            // as the climb goes on: the same stop rule level by level, since a
+            // batch's moves only shift entries below its top ancestor (a
+            // tenth of the pushes climb past four levels)
+            int c = cur;
+            for (;;) {
+                double ak[kUp];
+#pragma unroll
+                for (int j = 0; j < kUp; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
+                int m = 0;
+#pragma unroll
+                for (int j = 0; j < kUp; ++j)
+                    if (m == j && (c >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
+                if constexpr (kUp <= SVG_UP_ARRAY) {
+                    T mv[kUp];
+#pragma unroll
+                    for (int j = 0; j < kUp; ++j)
+                        if (j < m) mv[j] = H[c >> (j + 1)];
+#pragma unroll
+                    for (int j = 0; j < kUp; ++j)
+                        if (j < m) H[c >> j] = mv[j];
+                } else {
+                    for (int j = 0; j < m; ++j) H[c >> j] = H[c >> (j + 1)];
+                }
+                c >>= m;
+                if (m < kUp) break;
+            }
+            H[c] = x;
+            return c;
+#elif SVG_KEYS_ONLY_SIFT
             // keys of the first kUp ancestors in one round trip; the moved
             // entries are read again (their sectors were just fetched) before
             // each is written one level down
@@ -749,6 +784,7 @@ struct LaneT {
             for (int j = 0; j < 4; ++j)
                 if (j < m) H[cur >> j] = anc[j];
 #endif
+#if !(SVG_KEYS_ONLY_SIFT && SVG_UP_BATCHES)
             int c = cur >> m;
             if (m == kUp) {
                 for (;;) {
@@ -762,6 +798,7 @@ struct LaneT {
             }
             H[c] = x;
             return c;
+#endif
         }
     }
 
@@ -1034,8 +1071,25 @@ struct LaneT {
         if constexpr (kCoop) {
             sift_up(PH(), ++psize, e);
         } else if (SVG_PPUSH_SIFT) {
-            const int at = sift_up(PH(), ++psize, e);
-            if (at == 1) set_ptop(e);
+            // four ancestors' keys per round trip for as long as the climb
+            // goes on, the moves one entry at a time (the stop rule of the
+            // level-by-level loop below)
+            PsEntry* H = PH();
+            int c = ++psize;
+            for (;;) {
+                double ak[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
+                int m = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (m == j && (c >> (j + 1)) > 0 && ak[j] > key) m = j + 1;
+                for (int j = 0; j < m; ++j) H[c >> j] = H[c >> (j + 1)];
+                c >>= m;
+                if (m < 4) break;
+            }
+            H[c] = e;
+            if (c == 1) set_ptop(e);
         } else {
             int cur = ++psize, p = cur >> 1;
             while (p > 0) {
