@@ -57,6 +57,10 @@
 #ifndef SVG_UP_LEVELS
 #define SVG_UP_LEVELS 4
 #endif
+// keys-only sift-up: ancestors in its first batch (0: SVG_UP_LEVELS)
+#ifndef SVG_UP_FIRST
+#define SVG_UP_FIRST 0
+#endif
 // 1: the keys-only sift-up reads a further batch of ancestors' keys per round
 // trip while the climb goes on (0: one level per round trip past the first batch)
 #ifndef SVG_UP_BATCHES
@@ -101,8 +105,8 @@
 #ifndef SVG_TOP_CACHE
 #define SVG_TOP_CACHE 0
 #endif
-// 1: the one-thread pseudo-source push climbs with the window push's sift-up
-// (four ancestors per round trip); 0: level by level
+// 1: the one-thread pseudo-source push reads four ancestors' keys per round
+// trip; 0: level by level (measured 2-4 % faster)
 #ifndef SVG_PPUSH_SIFT
 #define SVG_PPUSH_SIFT 0
 #endif
@@ -718,15 +722,18 @@ struct LaneT {
             // as the climb goes on: the same stop rule level by level, since a
             // batch's moves only shift entries below its top ancestor (a
             // tenth of the pushes climb past four levels)
+            // (the first batch may be smaller: most pushes do not move)
+            constexpr int kFirst = SVG_UP_FIRST > 0 && SVG_UP_FIRST < kUp ? SVG_UP_FIRST : kUp;
             int c = cur;
-            for (;;) {
+            for (int batch = 0;; ++batch) {
+                const int nb = batch == 0 ? kFirst : kUp;
                 double ak[kUp];
 #pragma unroll
-                for (int j = 0; j < kUp; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
+                for (int j = 0; j < kUp; ++j) ak[j] = (j < nb && (c >> (j + 1)) > 0) ? H[c >> (j + 1)].key : 0.0;
                 int m = 0;
 #pragma unroll
                 for (int j = 0; j < kUp; ++j)
-                    if (m == j && (c >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
+                    if (j < nb && m == j && (c >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
                 if constexpr (kUp <= SVG_UP_ARRAY) {
                     T mv[kUp];
 #pragma unroll
@@ -739,7 +746,7 @@ struct LaneT {
                     for (int j = 0; j < m; ++j) H[c >> j] = H[c >> (j + 1)];
                 }
                 c >>= m;
-                if (m < kUp) break;
+                if (m < nb) break;
             }
             H[c] = x;
             return c;
