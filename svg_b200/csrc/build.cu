@@ -46,6 +46,10 @@
 #ifndef SVG_SPLIT_TRACE
 #define SVG_SPLIT_TRACE 1
 #endif
+// blocks of 256 per SM k_trace is compiled to fit (register budget)
+#ifndef SVG_TRACE_MIN_BLOCKS
+#define SVG_TRACE_MIN_BLOCKS 4
+#endif
 // threads per block the batched kernel is compiled for (the launch may use fewer)
 #ifndef SVG_ICH_TPB
 #define SVG_ICH_TPB 128
@@ -462,7 +466,7 @@ struct EmitParams {
 // (BuildGeodesicPathTo, ICHDevice.cu:336-480).  A walk is a chain of dependent
 // loads; run apart from the sort, with small blocks and few registers, many
 // more of them are in flight than inside k_emit's warps.
-__global__ void __launch_bounds__(256) k_trace(DevMesh M, PathEnd* path, int64_t nnz, int32_t* st_flags) {
+__global__ void __launch_bounds__(256, SVG_TRACE_MIN_BLOCKS) k_trace(DevMesh M, PathEnd* path, int64_t nnz, int32_t* st_flags) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
         PathEnd pe = path[e];
