@@ -961,6 +961,10 @@ def run_mixed(args):
     clocks.start()
     qrng = np.random.default_rng(5)
     res_ids, res_t = [], [0.0]
+    # host time of the submitting loop by call, and how late each submission was
+    host_s = {"submit_build": 0.0, "submit_query": 0.0, "resident": 0.0, "msad_slot_wait": 0.0, "stats": 0.0}
+    lag = []
+    bkw = {} if args.mixed_heavy_first < 0 else {"heavy_first": args.mixed_heavy_first}
     t0 = time.perf_counter()
     last_stats = t0
     for ta, kind, pl in ev:
@@ -970,38 +974,51 @@ def run_mixed(args):
             time.sleep(max(0.0, target - now - 0.0001))
             while time.perf_counter() < target:
                 pass
+        lag.append((time.perf_counter() - target) * 1e3)
         if kind == 2:
             mi, K = pl
-            gid, tk = srv.submit_build(meshes[mi], K)
+            tc = time.perf_counter()
+            gid, tk = srv.submit_build(meshes[mi], K, **bkw)
+            host_s["submit_build"] += time.perf_counter() - tc
             gid_mesh[gid] = mi
             with lock:
                 info[tk] = (2, gid)
             continue
         # the graphs resident now (refreshed every 20 ms)
+        tc = time.perf_counter()
         if time.perf_counter() - res_t[0] > 0.02 or not res_ids:
             res_ids[:] = srv.resident()
             res_t[0] = time.perf_counter()
         while not res_ids:   # nothing built yet: the query waits for the first graph
             time.sleep(0.001)
             res_ids[:] = srv.resident()
+        host_s["resident"] += time.perf_counter() - tc
         gids = res_ids
         gid = gids[int(qrng.integers(0, len(gids)))]
         V = Vs[gid_mesh[gid]]
         if kind == 0:
             a, b = qrng.integers(0, V, 2)
+            tc = time.perf_counter()
             tk = srv.submit_sssd(gid, int(a), int(b))
+            host_s["submit_query"] += time.perf_counter() - tc
         else:
             k = int(np.clip(np.rint(np.exp(qrng.uniform(0.0, np.log(1000.0)))), 1, 1000))
             srcs = np.unique(qrng.integers(0, V, k)).astype(np.int32)
+            tc = time.perf_counter()
             sl = ring_free.get(timeout=dur * 2 + 120)   # raises instead of waiting for good
+            host_s["msad_slot_wait"] += time.perf_counter() - tc
+            tc = time.perf_counter()
             tk = srv.submit_msad(gid, srcs, out=(ring_d[sl][:V], ring_s[sl][:V]))
+            host_s["submit_query"] += time.perf_counter() - tc
             with lock:
                 slot_of[tk] = sl
         with lock:
             info[tk] = (kind, gid)
         if time.perf_counter() - last_stats > 0.5:
+            tc = time.perf_counter()
             peak_res[0] = max(peak_res[0], srv.stats()["resident_bytes"])
             last_stats = time.perf_counter()
+            host_s["stats"] += last_stats - tc
     complete = finished.wait(dur * 2 + 120)
     wall = (t_done[0] if complete else time.perf_counter()) - t0
     ck = clocks.stop()
@@ -1025,7 +1042,11 @@ def run_mixed(args):
             "build_edges_per_s_device": be / (bms / 1e3) if bms > 0 else None,
             "builds_per_s": len(builds) / wall,
             "evictions": st["evictions"], "rebuilds": st["rebuilds"], "resident_graphs_end": st["resident_graphs"],
-            "peak_resident_bytes_sampled": peak_res[0], "clocks": ck}
+            "peak_resident_bytes_sampled": peak_res[0],
+            "submit_lag_ms": {"p50": _pct(lag, 50), "p99": _pct(lag, 99), "max": max(lag) if lag else None},
+            "submit_loop_host_s": {k: round(v, 3) for k, v in host_s.items()},
+            "build_heavy_first": "library default" if args.mixed_heavy_first < 0 else args.mixed_heavy_first,
+            "clocks": ck}
     emit(line, args)
     return 0
 
@@ -1064,6 +1085,8 @@ def main():
     ap.add_argument("--record", default="", help="also write the JSON line to this file")
     ap.add_argument("--no-autotune", action="store_true", help="time the default schedule, not the tuned one")
     ap.add_argument("--no-graph", action="store_true", help="timed builds without the captured CUDA graph")
+    ap.add_argument("--mixed-heavy-first", type=int, default=-1,
+                    help="mixed: heavy_first of the served builds (-1 = the library default)")
     ap.add_argument("--e2e-heavy-first", type=int, default=-1,
                     help="e2e: heavy_first of the fresh-mesh build (-1 = the library default)")
     ap.add_argument("--replicas", action="store_true",
