@@ -166,16 +166,13 @@ Request* oldest(svg_server* S, int kind) {
 
 bool graph_has_queued(const GraphEntry& G) { return !G.q[0].empty() || !G.q[1].empty(); }
 
-// Take a batch for a free lane off the queues and claim the lane for it
-// (busy, the graph in flight so that it is not evicted).  Called with S->mu
-// held; false if nothing is queued.  The lane's query context for the graph
-// is returned in ctx (null if it has none yet).
-bool take_batch(svg_server* S, Lane& L, svg_qctx*& ctx, svg_graph*& g) {
+// Launch a batch on a free lane.  Called with S->mu held.
+void launch_batch(svg_server* S, Lane& L) {
     // short requests first: the oldest SSSD, unless the oldest MSAD is older
     // than it and has waited past the age limit (MSAD cannot starve)
     Request* so = oldest(S, kSSSD);
     Request* mo = oldest(S, kMSAD);
-    if (!so && !mo) return false;
+    if (!so && !mo) return;
     Request* first = so ? so : mo;
     if (so && mo && mo->t_submit < so->t_submit && now_s() - mo->t_submit >= kMsadAgeLimit) first = mo;
     const int kind = first->kind, gi = first->graph;
@@ -183,7 +180,7 @@ bool take_batch(svg_server* S, Lane& L, svg_qctx*& ctx, svg_graph*& g) {
     const int V = G.g->nv;
     // gather the batch: oldest first, same kind and graph, within staging capacity
     std::vector<Request*> batch;
-    size_t in_used = 0, out_used = 0;
+    size_t in_used = 0, out_used = 0, nsrc = 0;
     const size_t max_n = (size_t)(kind == kSSSD ? S->o.max_batch : S->o.max_batch_msad);
     auto& gq = G.q[kind];  // this graph's queue of the kind: `first` is at its front
     while (!gq.empty() && batch.size() < max_n) {
@@ -207,35 +204,14 @@ bool take_batch(svg_server* S, Lane& L, svg_qctx*& ctx, svg_graph*& g) {
         }
         in_used += in_need;
         out_used += out_need;
+        nsrc += r->srcs.size();
         batch.push_back(r);
     }
-    if (batch.empty()) return false;
+    if (batch.empty()) return;
     L.batch = batch;  // owned by the lane from here on (reported failed if a launch step throws)
-    auto it = L.ctx.find(gi);
-    ctx = it == L.ctx.end() ? nullptr : it->second;
-    g = G.g;
-    L.busy = true;
-    L.kind = kind;
-    L.graph = gi;
-    L.nv = V;
-    L.t_launch = now_s();
-    G.inflight += 1;
-    G.last_used = L.t_launch;
-    S->batches += 1;
-    S->batched_requests += (int64_t)batch.size();
-    return true;
-}
-
-// Stage a taken batch's inputs, launch its search and the copy of its results
-// back, and record the lane's event.  Runs without the lock: the lane and its
-// batch belong to the worker until the event has completed, and the graph,
-// in flight, stays resident.
-void issue_batch(Lane& L, svg_qctx* ctx) {
-    const int kind = L.kind;
-    const int V = L.nv;
-    const std::vector<Request*>& batch = L.batch;
-    size_t nsrc = 0;
-    for (const Request* r : batch) nsrc += r->srcs.size();
+    // per-lane context for this graph
+    svg_qctx*& ctx = L.ctx[gi];
+    if (!ctx) ctx = qctx_create(G.g, S->slots, L.st, S->cluster);
     const int n = (int)batch.size();
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     if (kind == kSSSD) {
@@ -274,6 +250,15 @@ void issue_batch(Lane& L, svg_qctx* ctx) {
                                  L.st));
     }
     SVG_CUDA(cudaEventRecord(L.ev, L.st));
+    L.busy = true;
+    L.kind = kind;
+    L.graph = gi;
+    L.nv = V;
+    L.t_launch = now_s();
+    G.inflight += 1;
+    G.last_used = L.t_launch;
+    S->batches += 1;
+    S->batched_requests += n;
 }
 
 // Copy a finished batch's results out of the lane's pinned staging into the
@@ -323,36 +308,19 @@ void publish_batch(svg_server* S, Lane& L) {
     L.draining = false;
 }
 
-// Take a batch for lane L and launch it, the launch without the lock (a CUDA
-// call that waits, such as a first query context's set-up while a build
-// kernel holds the GPU, then does not hold up the threads that submit); its
-// failures are reported on the batch's requests.  Called with S->mu held (lk
-// owns it) and returns with it held; true if a batch was launched.
-bool launch_guarded(svg_server* S, Lane& L, std::unique_lock<std::mutex>& lk) {
-    svg_qctx* ctx = nullptr;
-    svg_graph* g = nullptr;
-    if (!take_batch(S, L, ctx, g)) return false;
-    svg_qctx* created = nullptr;
-    int code = SVG_OK;
-    std::string err;
-    lk.unlock();
+// launch_batch with its failures reported on the batch's requests.  Called
+// with S->mu held; true if a batch was launched.
+bool launch_guarded(svg_server* S, Lane& L) {
     try {
-        if (!ctx) ctx = created = qctx_create(g, S->slots, L.st, S->cluster);
-        issue_batch(L, ctx);
+        launch_batch(S, L);
+        return L.busy;
     } catch (const SvgError& e) {
-        code = e.code;
-        err = e.msg;
+        // the batch's requests were taken off the queues: report them failed
+        for (Request* r : L.batch) finish_request(S, r, e.code, e.msg);
     } catch (const CudaFail& e) {
         cudaGetLastError();
-        code = SVG_ERR_CUDA;
-        err = e.where;
+        for (Request* r : L.batch) finish_request(S, r, SVG_ERR_CUDA, e.where);
     }
-    lk.lock();
-    if (created) L.ctx[L.graph] = created;  // the graph is in flight: no rebuild replaced its contexts
-    if (code == SVG_OK) return true;
-    // the batch's requests were taken off the queues: report them failed
-    for (Request* r : L.batch) finish_request(S, r, code, err);
-    S->graphs[(size_t)L.graph].inflight -= 1;
     L.batch.clear();
     L.busy = false;
     return false;
@@ -360,37 +328,23 @@ bool launch_guarded(svg_server* S, Lane& L, std::unique_lock<std::mutex>& lk) {
 
 void worker_main(svg_server* S) {
     cudaSetDevice(S->dev);
-    std::vector<Lane*> polled;
-    std::vector<char> fin;
     std::unique_lock<std::mutex> lk(S->mu);
     while (!S->stop) {
         bool progressed = false;
-        // the busy lanes' events are polled without the lock: only this thread
-        // launches on a lane and marks it draining, so a busy lane keeps its
-        // batch and event meanwhile
-        polled.clear();
+        std::vector<Lane*> ready;
         for (auto& L : S->lanes)
-            if (L.busy && !L.draining) polled.push_back(&L);
-        if (!polled.empty()) {
-            lk.unlock();
-            fin.assign(polled.size(), 0);
-            for (size_t i = 0; i < polled.size(); ++i) fin[i] = cudaEventQuery(polled[i]->ev) == cudaSuccess;
-            lk.lock();
-        }
-        bool ready = false;
-        for (size_t i = 0; i < polled.size(); ++i)
-            if (fin[i]) {
-                polled[i]->draining = true;
-                S->copy_q.push_back(polled[i]);
-                ready = true;
+            if (L.busy && !L.draining && cudaEventQuery(L.ev) == cudaSuccess) {
+                L.draining = true;
+                ready.push_back(&L);
             }
-        if (ready) {
+        if (!ready.empty()) {
+            for (Lane* L : ready) S->copy_q.push_back(L);
             S->cv_copy.notify_all();
             progressed = true;
         }
         for (auto& L : S->lanes) {
             if (L.busy || S->queued.empty()) continue;
-            progressed |= launch_guarded(S, L, lk);
+            progressed |= launch_guarded(S, L);
         }
         bool any_busy = false;
         for (auto& L : S->lanes) any_busy |= L.busy;
