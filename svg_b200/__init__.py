@@ -508,6 +508,20 @@ class Server:
         _check(lib().svg_server_poll(self._h, max_n, C.cast(arr, _P), C.byref(n)))
         return [{k: getattr(arr[i], k) for k, _ in ServerResult._fields_} for i in range(n.value)]
 
+    _POLL_DT = np.dtype([("ticket", np.int64), ("status", np.int32), ("kind", np.int32), ("graph_id", np.int32),
+                         ("n", np.int32), ("latency_ms", np.float64), ("dist", np.float64), ("edges", np.int64),
+                         ("build_ms", np.float64)], align=True)
+
+    def poll_array(self, max_n: int = 4096) -> np.ndarray:
+        """svg_server_poll into a numpy structured array (the ServerResult
+        fields), without a Python object per field: for callers that drain
+        thousands of results a second."""
+        assert self._POLL_DT.itemsize == C.sizeof(ServerResult)
+        out = np.empty(max_n, self._POLL_DT)
+        n = C.c_int32()
+        _check(lib().svg_server_poll(self._h, max_n, out.ctypes.data_as(_P), C.byref(n)))
+        return out[:n.value]
+
     def resident(self, max_n: int = 4096) -> list:
         """Graph ids resident now, most recently used first."""
         ids = np.zeros(max_n, np.int32)
