@@ -477,12 +477,6 @@ void builder_main(svg_server* S) {
             continue;
         }
         o.hbm_budget = std::max<int64_t>(S->o.hbm_budget - S->resident_bytes - est_graph - est_ctx, scratch);
-        // no K/10 probe build on the serving GPU: the graph's first build runs
-        // in vertex order, its rebuilds heaviest first by the costs the mesh
-        // recorded (measured on the mixed workload: with the probe 1,357
-        // queries/s and the submitting loop up to 31 s behind its schedule,
-        // without it 1,888 queries/s)
-        if (o.heavy_first == 2) o.heavy_first = 1;
         if (o.blocks <= 0 && S->o.build_blocks_per_sm > 0) o.blocks = S->sms * S->o.build_blocks_per_sm;
         svg_graph* g = nullptr;
         lk.unlock();
