@@ -42,10 +42,6 @@
 #ifndef SVG_ICH_INLINE_STALE
 #define SVG_ICH_INLINE_STALE 8
 #endif
-// 1: peek() prefetches into L1 the face records the next window step reads
-#ifndef SVG_FACE_PREFETCH
-#define SVG_FACE_PREFETCH 0
-#endif
 // 1: the one-thread sifts prefetch keys only and re-read the moved entries;
 // 0: they prefetch whole entries (one L1 round trip fewer per move).  With the
 // three-level sift-down below, keys only measured 1.3 % faster (the sift-up
@@ -57,10 +53,6 @@
 #ifndef SVG_UP_LEVELS
 #define SVG_UP_LEVELS 4
 #endif
-// keys-only sift-up: ancestors in its first batch (0: SVG_UP_LEVELS)
-#ifndef SVG_UP_FIRST
-#define SVG_UP_FIRST 0
-#endif
 // 1: the keys-only sift-up reads a further batch of ancestors' keys per round
 // trip while the climb goes on (0: one level per round trip past the first batch)
 #ifndef SVG_UP_BATCHES
@@ -70,11 +62,6 @@
 // into registers together and then written; beyond it, one at a time
 #ifndef SVG_UP_ARRAY
 #define SVG_UP_ARRAY 4
-#endif
-// 1: the one-thread sift-down reads the keys of four levels per round trip
-// (overrides SVG_SIFT3)
-#ifndef SVG_SIFT4
-#define SVG_SIFT4 0
 #endif
 // 1: the one-thread sift-down reads the keys of three levels per round trip
 // (measured 2.6 % faster on the 72.9K height field at K = 500, 4 % on the
@@ -87,49 +74,21 @@
 #ifndef SVG_FREE_CACHE
 #define SVG_FREE_CACHE 1
 #endif
-// 1: the pseudo-source fan walks load the next half-edge records before the
-// current one's push or table probe (measured 3 % slower: off)
-#ifndef SVG_FAN_PIPE
-#define SVG_FAN_PIPE 0
-#endif
 // 1: a lane's counters and its cached look at the heap tops live in shared
 // memory (one slot per thread, structure of arrays) instead of registers
 // (measured 3-4 % faster)
 #ifndef SVG_SMEM_STATE
 #define SVG_SMEM_STATE 1
 #endif
-// 1: the lane keeps copies of its two heap tops, updated by every push and
-// pop (a pop's sift-down reads the new top anyway), so a look at the tops
-// needs no load.  Measured 5 % slower: the top's load hits L1 and the copies
-// cost registers (or shared-memory traffic).  Off.
-#ifndef SVG_TOP_CACHE
-#define SVG_TOP_CACHE 0
-#endif
-// 1: the one-thread pseudo-source push reads four ancestors' keys per round
-// trip; 0: level by level (measured 2-4 % faster)
-#ifndef SVG_PPUSH_SIFT
-#define SVG_PPUSH_SIFT 0
-#endif
 // 1: propagate() inserts a missing vertex or split entry at the empty slot its
 // lookup ended on (no second probe walk; measured 2-4.5 % faster)
 #ifndef SVG_INSERT_AT
 #define SVG_INSERT_AT 1
 #endif
-// 1: propagate() prefetches into L1 the heap slots its pushes read first
-// (measured no faster: off); 2: into L2
-#ifndef SVG_PUSH_PREFETCH
-#define SVG_PUSH_PREFETCH 0
-#endif
 // 1: propagate() builds, tests and pushes one child window at a time through
 // one copy of the code (fewer live registers; measured 10 % faster)
 #ifndef SVG_SEQ_CHILD
 #define SVG_SEQ_CHILD 1
-#endif
-// 1: the vertex ids of the top window's face are loaded before its pop's
-// sift-down, so propagate() issues its table probes with the face loads
-// (measured no faster: off)
-#ifndef SVG_FACE_IDS
-#define SVG_FACE_IDS 0
 #endif
 
 namespace svgb {
@@ -381,15 +340,8 @@ struct LaneSmem {
     double pkey[128];
     int32_t pvert[128];
     uint32_t plb[128];
-    int32_t cross[128];
     int32_t windows[128], pseudos[128], generated[128], maxw[128], maxp[128];
     long long steps[128];
-    double twkey[128];  // heap tops (SVG_TOP_CACHE)
-    int32_t twpsrc[128];
-    uint32_t twsb[128];
-    double tpkey[128];
-    int32_t tpvert[128];
-    uint32_t tplb[128];
 };
 __shared__ LaneSmem g_lane_smem;
 #endif
@@ -419,42 +371,6 @@ struct LaneT {
     __device__ __forceinline__ VSlot* VT() const { return C.vtab + ((size_t)lid << C.vcap_log2); }
     __device__ __forceinline__ int32_t* VL() const { return C.vlist + (size_t)lid * C.vlimit; }
     __device__ __forceinline__ SSlot* ST() const { return C.stab + ((size_t)lid << C.scap_log2); }
-    // Heap tops (SVG_TOP_CACHE, one-thread form): equal to WH()[1] / PH()[1]
-    // whenever the heap is not empty.
-#if SVG_TOP_CACHE && SVG_SMEM_STATE
-    __device__ __forceinline__ void set_wtop(const WinEntry& e) const {
-        const int t = threadIdx.x;
-        g_lane_smem.twkey[t] = e.key; g_lane_smem.twpsrc[t] = e.psrc; g_lane_smem.twsb[t] = e.sb;
-    }
-    __device__ __forceinline__ void set_ptop(const PsEntry& e) const {
-        const int t = threadIdx.x;
-        g_lane_smem.tpkey[t] = e.key; g_lane_smem.tpvert[t] = e.vert; g_lane_smem.tplb[t] = e.lb;
-    }
-    __device__ __forceinline__ WinEntry wtop() const {
-        const int t = threadIdx.x;
-        WinEntry e;
-        e.key = g_lane_smem.twkey[t]; e.psrc = g_lane_smem.twpsrc[t]; e.sb = g_lane_smem.twsb[t];
-        return e;
-    }
-    __device__ __forceinline__ PsEntry ptop() const {
-        const int t = threadIdx.x;
-        PsEntry e;
-        e.key = g_lane_smem.tpkey[t]; e.vert = g_lane_smem.tpvert[t]; e.lb = g_lane_smem.tplb[t];
-        return e;
-    }
-#elif SVG_TOP_CACHE
-    WinEntry tw_;
-    PsEntry tp_;
-    __device__ __forceinline__ void set_wtop(const WinEntry& e) { tw_ = e; }
-    __device__ __forceinline__ void set_ptop(const PsEntry& e) { tp_ = e; }
-    __device__ __forceinline__ WinEntry wtop() const { return tw_; }
-    __device__ __forceinline__ PsEntry ptop() const { return tp_; }
-#else
-    __device__ __forceinline__ void set_wtop(const WinEntry&) const {}
-    __device__ __forceinline__ void set_ptop(const PsEntry&) const {}
-    __device__ __forceinline__ WinEntry wtop() const { return WH()[1]; }
-    __device__ __forceinline__ PsEntry ptop() const { return PH()[1]; }
-#endif
     int wsize, psize, nfree, nfresh;
     int ftop;       // WF()[nfree - 1] when nfree > 0 (free-slot cache)
     int vcount, scount;
@@ -722,18 +638,15 @@ struct LaneT {
             // as the climb goes on: the same stop rule level by level, since a
             // batch's moves only shift entries below its top ancestor (a
             // tenth of the pushes climb past four levels)
-            // (the first batch may be smaller: most pushes do not move)
-            constexpr int kFirst = SVG_UP_FIRST > 0 && SVG_UP_FIRST < kUp ? SVG_UP_FIRST : kUp;
             int c = cur;
-            for (int batch = 0;; ++batch) {
-                const int nb = batch == 0 ? kFirst : kUp;
+            for (;;) {
                 double ak[kUp];
 #pragma unroll
-                for (int j = 0; j < kUp; ++j) ak[j] = (j < nb && (c >> (j + 1)) > 0) ? H[c >> (j + 1)].key : 0.0;
+                for (int j = 0; j < kUp; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
                 int m = 0;
 #pragma unroll
                 for (int j = 0; j < kUp; ++j)
-                    if (j < nb && m == j && (c >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
+                    if (m == j && (c >> (j + 1)) > 0 && ak[j] > x.key) m = j + 1;
                 if constexpr (kUp <= SVG_UP_ARRAY) {
                     T mv[kUp];
 #pragma unroll
@@ -746,7 +659,7 @@ struct LaneT {
                     for (int j = 0; j < m; ++j) H[c >> j] = H[c >> (j + 1)];
                 }
                 c >>= m;
-                if (m < nb) break;
+                if (m < kUp) break;
             }
             H[c] = x;
             return c;
@@ -838,8 +751,7 @@ struct LaneT {
         e.key = w.key;
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        const int at = sift_up(WH(), ++wsize, e);
-        if (at == 1) set_wtop(e);
+        sift_up(WH(), ++wsize, e);
         if (wsize > st_maxw()) st_maxw() = wsize;
     }
     // Cooperative sift-down: the 62 nodes 1-5 levels below `cur` are loaded
@@ -895,80 +807,13 @@ struct LaneT {
     // again from the sectors just fetched and written with predicated stores,
     // one exit test per two levels.
     template <class T>
-    // nt receives the heap's new top entry (its root after the sift).
-    __device__ __forceinline__ int sift_down2(T* H, int n, const T& last, T& nt) {
-        nt = last;
+    __device__ __forceinline__ int sift_down2(T* H, int n, const T& last) {
         if constexpr (kCoop) return coop_sift_down(H, n, last);
         int cur = 1;
         for (;;) {
             const int l = cur << 1;
             if (l > n) break;
-#if SVG_SIFT4
-            // keys of four levels below cur (2 + 4 + 8 + 16) in one round trip
-            // (reads past the heap's end stay inside the lane's array, stride
-            // >= cap + 16, and are never used); the moved entries are read
-            // again from the sectors just fetched
-            const double a = H[l].key, b = H[l + 1].key;
-            const int g = cur << 2, h8 = cur << 3, h16 = cur << 4;
-            double q[4], r[8], t[16];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) q[i] = 0.0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) r[i] = 0.0;
-#pragma unroll
-            for (int i = 0; i < 16; ++i) t[i] = 0.0;
-            if (g <= n) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) q[i] = H[g + i].key;
-            }
-            if (h8 <= n) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i) r[i] = H[h8 + i].key;
-            }
-            if (h16 <= n) {
-#pragma unroll
-                for (int i = 0; i < 16; ++i) t[i] = H[h16 + i].key;
-            }
-            const int k1 = (l + 1 <= n && !(a < b)) ? 1 : 0;
-            const bool mv1 = (k1 ? b : a) < last.key;
-            const int c1 = l + k1;
-            const int l2 = c1 << 1;
-            const double a2 = k1 ? q[2] : q[0], b2 = k1 ? q[3] : q[1];
-            const int k2 = (l2 + 1 <= n && !(a2 < b2)) ? 1 : 0;
-            const bool mv2 = mv1 && l2 <= n && (k2 ? b2 : a2) < last.key;
-            const int c2 = l2 + k2;
-            const int l3 = c2 << 1;  // = h8 + 4 k1 + 2 k2
-            const double a3 = k1 ? (k2 ? r[6] : r[4]) : (k2 ? r[2] : r[0]);
-            const double b3 = k1 ? (k2 ? r[7] : r[5]) : (k2 ? r[3] : r[1]);
-            const int k3 = (l3 + 1 <= n && !(a3 < b3)) ? 1 : 0;
-            const bool mv3 = mv2 && l3 <= n && (k3 ? b3 : a3) < last.key;
-            const int c3 = l3 + k3;
-            const int l4 = c3 << 1;  // = h16 + 8 k1 + 4 k2 + 2 k3
-            double ua[4], ub[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                ua[i] = k1 ? t[8 + 2 * i] : t[2 * i];
-                ub[i] = k1 ? t[9 + 2 * i] : t[2 * i + 1];
-            }
-            const double va0 = k2 ? ua[2] : ua[0], va1 = k2 ? ua[3] : ua[1];
-            const double vb0 = k2 ? ub[2] : ub[0], vb1 = k2 ? ub[3] : ub[1];
-            const double a4 = k3 ? va1 : va0, b4 = k3 ? vb1 : vb0;
-            const int k4 = (l4 + 1 <= n && !(a4 < b4)) ? 1 : 0;
-            const bool mv4 = mv3 && l4 <= n && (k4 ? b4 : a4) < last.key;
-            const int c4 = l4 + k4;
-            T e1, e2, e3, e4;
-            if (mv1) e1 = H[c1];
-            if (mv2) e2 = H[c2];
-            if (mv3) e3 = H[c3];
-            if (mv4) e4 = H[c4];
-            if (l == 2 && mv1) nt = e1;
-            if (mv1) H[cur] = e1;
-            if (mv2) H[c1] = e2;
-            if (mv3) H[c2] = e3;
-            if (mv4) H[c3] = e4;
-            cur = mv4 ? c4 : (mv3 ? c3 : (mv2 ? c2 : (mv1 ? c1 : cur)));
-            const bool more = mv4;
-#elif SVG_SIFT3
+#if SVG_SIFT3
             // keys of three levels below cur (2 + 4 + 8) in one round trip
             // (reads past the heap's end stay inside the lane's array,
             // stride >= cap + 16, and are never used); the moved entries are
@@ -1000,7 +845,6 @@ struct LaneT {
             if (mv1) e1 = H[c1];
             if (mv2) e2 = H[c2];
             if (mv3) e3 = H[c3];
-            if (l == 2 && mv1) nt = e1;
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             if (mv3) H[c2] = e3;
@@ -1022,7 +866,6 @@ struct LaneT {
             T e1, e2;
             if (mv1) e1 = H[c1];
             if (mv2) e2 = H[c2];
-            if (l == 2 && mv1) nt = e1;
             if (mv1) H[cur] = e1;
             if (mv2) H[c1] = e2;
             cur = mv2 ? c2 : (mv1 ? c1 : cur);
@@ -1035,7 +878,6 @@ struct LaneT {
             const int k1 = (l + 1 <= n && !(a.key < b.key)) ? 1 : 0;
             const T e1 = k1 ? b : a;
             const bool mv1 = e1.key < last.key;
-            if (l == 2 && mv1) nt = e1;
             const int c1 = l + k1;
             const int l2 = c1 << 1;
             const T a2 = k1 ? q2 : q0, b2 = k1 ? q3 : q1;
@@ -1052,13 +894,11 @@ struct LaneT {
         return cur;
     }
     __device__ WinEntry wpop() {
-        const WinEntry top = (SVG_TOP_CACHE && !kCoop) ? wtop() : WH()[1];
+        const WinEntry top = WH()[1];
         WinEntry last = WH()[wsize];
         const int n = --wsize;
-        WinEntry nt;
-        const int cur = sift_down2(WH(), n, last, nt);
+        const int cur = sift_down2(WH(), n, last);
         WH()[cur] = last;
-        set_wtop(nt);
         WF()[nfree++] = (uint16_t)(top.sb & 0xFFFF);
         ftop = (int)(top.sb & 0xFFFF);
         if constexpr (kCoop) __syncwarp();
@@ -1077,26 +917,6 @@ struct LaneT {
         e.key = key; e.vert = vert; e.lb = ((uint32_t)level << 8) | (uint32_t)(birth & 0xFF);
         if constexpr (kCoop) {
             sift_up(PH(), ++psize, e);
-        } else if (SVG_PPUSH_SIFT) {
-            // four ancestors' keys per round trip for as long as the climb
-            // goes on, the moves one entry at a time (the stop rule of the
-            // level-by-level loop below)
-            PsEntry* H = PH();
-            int c = ++psize;
-            for (;;) {
-                double ak[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
-                int m = 0;
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (m == j && (c >> (j + 1)) > 0 && ak[j] > key) m = j + 1;
-                for (int j = 0; j < m; ++j) H[c >> j] = H[c >> (j + 1)];
-                c >>= m;
-                if (m < 4) break;
-            }
-            H[c] = e;
-            if (c == 1) set_ptop(e);
         } else {
             int cur = ++psize, p = cur >> 1;
             while (p > 0) {
@@ -1107,18 +927,15 @@ struct LaneT {
                 p = cur >> 1;
             }
             ph(cur) = e;
-            if (cur == 1) set_ptop(e);
         }
         if (psize > st_maxp()) st_maxp() = psize;
     }
     __device__ PsEntry ppop() {
-        const PsEntry top = (SVG_TOP_CACHE && !kCoop) ? ptop() : PH()[1];
+        const PsEntry top = PH()[1];
         PsEntry last = PH()[psize];
         const int n = --psize;
-        PsEntry nt;
-        const int cur = sift_down2(PH(), n, last, nt);
+        const int cur = sift_down2(PH(), n, last);
         PH()[cur] = last;
-        set_ptop(nt);
         if constexpr (kCoop) __syncwarp();
         return top;
     }
@@ -1247,9 +1064,7 @@ struct LaneT {
     // All lanes of `amask` call this together and meet at each __syncwarp, so
     // the phases run converged; a lane with nothing to do (live == false, or a
     // boundary edge, or a full table) only predicates its work off.
-    // fid: the face's vertex ids (h0.v0, h0.v1, h1.v1) when loaded ahead
-    // (SVG_FACE_IDS), else unused
-    __device__ void propagate(const WinPay& win, int psrc, int birth, bool live, unsigned amask, const int3& fid) {
+    __device__ void propagate(const WinPay& win, int psrc, int birth, bool live, unsigned amask) {
         const DevMesh& M = C.M;
         const int e0 = win.cross;
         live = live && e0 != -1;
@@ -1270,40 +1085,14 @@ struct LaneT {
             v2 = ld_apex(M.geo, e0);
             top1 = ld_top(M.geo, e1);
             top2 = ld_top(M.geo, e2);
-#if SVG_FACE_IDS
-            A = fid.x;
-            B = fid.y;
-            Cv = fid.z;
-#else
             A = h0.v0;
             B = h0.v1;
             Cv = h1.v1;
-#endif
             if constexpr (!kCoop) {
                 vfirst(A, hA, kA, dA);
                 vfirst(B, hB, kB, dB);
                 vfirst(Cv, hC, kC, dC);
                 sfirst(e0, hS, kS, sdx);
-#if SVG_PUSH_PREFETCH
-                // the heap slots the children's sift-ups read first: the
-                // ancestors of positions wsize + 1 and wsize + 2, into L1
-                // while the probes are in flight
-                {
-                    const WinEntry* H = WH();
-                    const int p1 = wsize + 1, p2 = wsize + 2;
-#pragma unroll
-                    for (int j = 1; j <= 4; ++j) {
-                        if ((p1 >> j) > 0) {
-                            if (SVG_PUSH_PREFETCH == 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(H + (p1 >> j)));
-                            else asm volatile("prefetch.global.L1 [%0];" ::"l"(H + (p1 >> j)));
-                        }
-                    }
-                    if ((p2 >> 1) != (p1 >> 1)) {
-                        if (SVG_PUSH_PREFETCH == 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(H + (p2 >> 1)));
-                        else asm volatile("prefetch.global.L1 [%0];" ::"l"(H + (p2 >> 1)));
-                    }
-                }
-#endif
                 vfinish(A, hA, kA, dA);
                 vfinish(B, hB, kB, dB);
                 sC = vfinish(Cv, hC, kC, dC);
@@ -1499,39 +1288,6 @@ struct LaneT {
             if (flags & kFlagWatchdog) live = false;
         }
         __syncwarp(amask);
-#if SVG_FAN_PIPE
-        // The same walk with the next face's records loaded before this
-        // face's push, so the two round trips overlap.
-        if (live) {
-            int guard = 0;
-            int se = startEdge;
-            HeRec hs, hw, hn;
-            if (se >= 0) {
-                const int we = nxt(se);
-                hs = ld_he(M.he, se); hw = ld_he(M.he, we); hn = ld_he(M.he, nxt(we));
-            }
-            for (;;) {
-                if (se < 0) {  // the reference reads edges[-1] here
-                    flags |= kFlagUndefined;
-                    break;
-                }
-                NewWin w;
-                finish_window(0.0, hw.len, hs.len, hn.len, pdist, w);
-                w.p.cross = hw.twin;
-                w.p.level = plevel + 1;
-                const int nse = hn.twin;
-                const bool more = nse != endEdge;
-                if (more && nse >= 0) {
-                    const int we = nxt(nse);
-                    hs = ld_he(M.he, nse); hw = ld_he(M.he, we); hn = ld_he(M.he, nxt(we));
-                }
-                wpush(w, pv, pbirth);
-                se = nse;
-                if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
-                if (!more) break;
-            }
-        }
-#else
         if (live) {
             int guard = 0;
             do {
@@ -1551,28 +1307,13 @@ struct LaneT {
                 if (++guard > 1 << 20) { flags |= kFlagWatchdog; live = false; break; }
             } while (startEdge != endEdge);
         }
-#endif
         __syncwarp(amask);
         if (live) {
             int start = __ldg(&M.vr[pv].first), cur = start;
             int guard = 0;
-#if SVG_FAN_PIPE
-            // each half-edge record is loaded one iteration ahead, beside the
-            // current neighbour's table probe
-            HeRec hn = ld_he(M.he, cur);
-#endif
             do {
                 if (++guard > 1 << 20) { flags |= kFlagWatchdog; break; }
-#if SVG_FAN_PIPE
-                const HeRec hc = hn;
-                {
-                    int nc = hc.twin;
-                    if (nc != -1) nc = nxt(nc);
-                    if (nc != start && nc != -1) hn = ld_he(M.he, nc);
-                }
-#else
                 HeRec hc = ld_he(M.he, cur);
-#endif
                 int opv = hc.v1;
                 int os = vfind(opv);
                 double od = os < 0 ? DBL_MAX : VT()[os].dist;
@@ -1632,17 +1373,12 @@ struct LaneT {
         p.key = g_lane_smem.pkey[t]; p.vert = g_lane_smem.pvert[t]; p.lb = g_lane_smem.plb[t];
         return p;
     }
-    __device__ __forceinline__ void set_pk_cross(int c) const { g_lane_smem.cross[threadIdx.x] = c; }
-    __device__ __forceinline__ int pk_cross() const { return g_lane_smem.cross[threadIdx.x]; }
 #else
     WinEntry pkw_;
     PsEntry pkp_;
-    int pkc_;  // the top window's half-edge (-1: none or boundary)
     __device__ __forceinline__ void set_pk(const WinEntry& w, const PsEntry& p) { pkw_ = w; pkp_ = p; }
     __device__ __forceinline__ WinEntry pk_w() const { return pkw_; }
     __device__ __forceinline__ PsEntry pk_p() const { return pkp_; }
-    __device__ __forceinline__ void set_pk_cross(int c) { pkc_ = c; }
-    __device__ __forceinline__ int pk_cross() const { return pkc_; }
 #endif
 
     // Up to this many outdated tops (pseudo-source reborn since the entry was
@@ -1663,22 +1399,6 @@ struct LaneT {
         }
     }
 
-    // L1 prefetch of the records propagate() reads for a window crossing
-    // half-edge e0: the three half-edges of its face and their unfolded
-    // geometry (one 32-byte sector each).  The window is popped and propagated
-    // after the warp's vote and the sift-down; by then these are in L1
-    // instead of a DRAM round trip away.  A prefetch has no result and no
-    // fault, so a window that turns out stale costs six sector reads.
-    __device__ __forceinline__ void prefetch_face(int e0) const {
-        const int e1 = nxt(e0), e2 = nxt(e1);
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e0));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e1));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.he + e2));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e0));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e1));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(C.M.geo + e2));
-    }
-
     __device__ int peek_once() {
         pk_proc = false;
         if (done || (wsize == 0 && psize == 0) || (flags & (kFlagCapacity | kFlagWatchdog | kFlagUndefined))) {
@@ -1694,47 +1414,28 @@ struct LaneT {
         PsEntry pp;
         pw.key = 0.0; pw.psrc = 0; pw.sb = 0;
         pp.key = 0.0; pp.vert = 0; pp.lb = 0;
-        if (SVG_TOP_CACHE && !kCoop) {
-            if (wsize > 0) pw = wtop();
-            if (psize > 0) pp = ptop();
-        } else {
-            if (wsize > 0) pw = WH()[1];
-            if (psize > 0) pp = PH()[1];
-        }
+        if (wsize > 0) pw = WH()[1];
+        if (psize > 0) pp = PH()[1];
         set_pk(pw, pp);
         // both birth lookups issued together
         const bool wlook = wsize > 0 && pw.psrc != source;
         const bool plook = psize > 0;
         int wb = src_birth, pb = -1;
         if constexpr (kCoop) {
-            // the top window's half-edge, loaded before the probe's round trip
-            const int cross = wsize > 0 ? WP()[pw.sb & 0xFFFF].cross : -1;
-            set_pk_cross(cross);
             ProbeR rw, rp, r2, r3;
             coop_probe4(probe_q(VT(), C.vcap_log2, (uint32_t)pw.psrc, wlook),
                         probe_q(VT(), C.vcap_log2, (uint32_t)pp.vert, plook), probe_off(), probe_off(), epoch, rw,
                         rp, r2, r3);
             if (wlook) wb = rw.slot < 0 ? -1 : rw.head.w;
             if (plook) pb = rp.slot < 0 ? -1 : rp.head.w;
-            if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
         } else {
             uint32_t hw = 0, hp = 0;
             int4 kw = make_int4(0, 0, 0, 0), kp = make_int4(0, 0, 0, 0);
             double dw = 0.0, dp = 0.0;
             if (wlook) vfirst(pw.psrc, hw, kw, dw);
             if (plook) vfirst(pp.vert, hp, kp, dp);
-            // the top window's half-edge, loaded in the same round trip as the
-            // birth probes (its sector is the payload's, read again when the
-            // window is popped)
-#if SVG_FACE_IDS || SVG_FACE_PREFETCH
-            const int cross = wsize > 0 ? WP()[pw.sb & 0xFFFF].cross : -1;
-            set_pk_cross(cross);
-#else
-            const int cross = -1;
-#endif
             if (wlook) wb = vfinish(pw.psrc, hw, kw, dw) < 0 ? -1 : kw.w;
             if (plook) pb = vfinish(pp.vert, hp, kp, dp) < 0 ? -1 : kp.w;
-            if (SVG_FACE_PREFETCH && cross >= 0) prefetch_face(cross);
         }
         const bool wstale = wsize > 0 && (int)(signed char)(pw.sb >> 16) != wb;
         if (wstale) return pk_act = kActWindow;
@@ -1758,22 +1459,11 @@ struct LaneT {
         pay.cross = -1;
         pay.level = 0;
         if (proc) pay = WP()[t.sb & 0xFFFF];  // issued before the sift-down
-        int3 fid = make_int3(0, 0, 0);
-#if SVG_FACE_IDS
-        // the face's vertex ids, also issued before the sift-down (the
-        // half-edge is the payload's, read by peek())
-        const int pc = pk_cross();
-        if (proc && pc >= 0) {
-            const int4 a0 = __ldg(reinterpret_cast<const int4*>(C.M.he + pc));
-            const int4 a1 = __ldg(reinterpret_cast<const int4*>(C.M.he + nxt(pc)));
-            fid = make_int3(a0.x, a0.y, a1.y);
-        }
-#endif
         wpop();
         __syncwarp(amask);
         const bool live = proc && !(pay.level > C.M.nf);
         if (live) ++st_windows();
-        propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask, fid);
+        propagate(pay, t.psrc, (int)(signed char)(t.sb >> 16), live, amask);
         if (live && C.K != -1 && total >= C.K) done = true;
     }
 
