@@ -83,7 +83,7 @@
 // 1: propagate() loads the keys of its first push's ancestors with its table
 // probes (the push then skips its first round trip)
 #ifndef SVG_PUSH_PRELOAD
-#define SVG_PUSH_PRELOAD 0
+#define SVG_PUSH_PRELOAD 1
 #endif
 // 1: propagate() inserts a missing vertex or split entry at the empty slot its
 // lookup ended on (no second probe walk; measured 2-4.5 % faster)
