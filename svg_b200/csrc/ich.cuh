@@ -80,11 +80,6 @@
 #ifndef SVG_SMEM_STATE
 #define SVG_SMEM_STATE 1
 #endif
-// 1: propagate() loads the keys of its first push's ancestors with its table
-// probes (the push then skips its first round trip)
-#ifndef SVG_PUSH_PRELOAD
-#define SVG_PUSH_PRELOAD 0
-#endif
 // 1: propagate() inserts a missing vertex or split entry at the empty slot its
 // lookup ended on (no second probe walk; measured 2-4.5 % faster)
 #ifndef SVG_INSERT_AT
@@ -350,13 +345,6 @@ struct LaneSmem {
 };
 __shared__ LaneSmem g_lane_smem;
 #endif
-
-// Keys of a heap position's first four ancestors, loaded ahead of a push
-// (valid: still current when the push comes).
-struct Keys4 {
-    double k[4];
-    bool valid;
-};
 
 template <bool kCoop>
 struct LaneT {
@@ -628,7 +616,7 @@ struct LaneT {
     // no data-dependent branch splits the lanes; a higher climb continues level
     // by level.
     template <class T>
-    __device__ __forceinline__ int sift_up(T* H, int cur, const T& x, const Keys4& pre = Keys4{{0.0, 0.0, 0.0, 0.0}, false}) {
+    __device__ __forceinline__ int sift_up(T* H, int cur, const T& x) {
         if constexpr (kCoop) {
             // thread j holds ancestor cur >> (j + 1); the moves are the
             // ancestors, from the parent up, whose key exceeds x's
@@ -651,15 +639,10 @@ struct LaneT {
             // batch's moves only shift entries below its top ancestor (a
             // tenth of the pushes climb past four levels)
             int c = cur;
-            for (int batch = 0;; ++batch) {
+            for (;;) {
                 double ak[kUp];
-                if (kUp == 4 && batch == 0 && pre.valid) {  // the first batch's keys, loaded ahead
 #pragma unroll
-                    for (int j = 0; j < kUp; ++j) ak[j] = pre.k[j & 3];
-                } else {
-#pragma unroll
-                    for (int j = 0; j < kUp; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
-                }
+                for (int j = 0; j < kUp; ++j) ak[j] = (c >> (j + 1)) > 0 ? H[c >> (j + 1)].key : 0.0;
                 int m = 0;
 #pragma unroll
                 for (int j = 0; j < kUp; ++j)
@@ -740,7 +723,7 @@ struct LaneT {
     }
 
     // Push (PriorityQueue.cuh:48-67).
-    __device__ void wpush(const NewWin& w, int psrc, int birth, const Keys4& pre = Keys4{{0.0, 0.0, 0.0, 0.0}, false}) {
+    __device__ void wpush(const NewWin& w, int psrc, int birth) {
         ++st_generated();  // counts attempts, like numOfWinGen
         if (wsize >= C.wcap) {  // PriorityQueue.cuh:53: dropped when full
             flags |= kFlagQueueDrop;
@@ -768,7 +751,7 @@ struct LaneT {
         e.key = w.key;
         e.psrc = psrc;
         e.sb = (uint32_t)slot | ((uint32_t)(birth & 0xFF) << 16);
-        sift_up(WH(), ++wsize, e, pre);
+        sift_up(WH(), ++wsize, e);
         if (wsize > st_maxw()) st_maxw() = wsize;
     }
     // Cooperative sift-down: the 62 nodes 1-5 levels below `cur` are loaded
@@ -1093,7 +1076,6 @@ struct LaneT {
         double dA = 0.0, dB = 0.0, dC = 0.0;
         double2 sdx = v2;
         int sC = -1, sS = -1;
-        Keys4 pre{{0.0, 0.0, 0.0, 0.0}, false};
         if (live) {
             e1 = nxt(e0);
             e2 = nxt(e1);
@@ -1111,16 +1093,6 @@ struct LaneT {
                 vfirst(B, hB, kB, dB);
                 vfirst(Cv, hC, kC, dC);
                 sfirst(e0, hS, kS, sdx);
-#if SVG_PUSH_PRELOAD
-                // the first push's ancestors (position wsize + 1), in the
-                // same round trip as the probes
-                {
-                    const int p1 = wsize + 1;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) pre.k[j] = (p1 >> (j + 1)) > 0 ? WH()[p1 >> (j + 1)].key : 0.0;
-                    pre.valid = true;
-                }
-#endif
                 vfinish(A, hA, kA, dA);
                 vfinish(B, hB, kB, dB);
                 sC = vfinish(Cv, hC, kC, dC);
@@ -1226,10 +1198,7 @@ struct LaneT {
                             : valid_window(W, false, dC, dA, dB, elen, top2.x, top2.y);
             }
             __syncwarp(amask);
-            if (keep) {
-                wpush(W, psrc, birth, pre);
-                pre.valid = false;  // the heap changed below the next position's ancestors
-            }
+            if (keep) wpush(W, psrc, birth);
             __syncwarp(amask);
         }
     }
