@@ -607,14 +607,14 @@ struct LaneT {
 
     // ----------------------------------------------------------- heaps
     // The reference's sift-up (PriorityQueue.cuh:57-64): the new entry moves up
-    // while its parent's key is greater.  New windows lie just behind the
-    // propagation front, so their keys are among the smallest in the heap and
-    // they usually climb far.  The first four ancestors are loaded in one
-    // round trip (they are what the level-by-level loop would read: a move
-    // only writes below the next ancestor); the number of moves over them is
-    // counted with the same stop rule and the moves are written predicated, so
-    // no data-dependent branch splits the lanes; a higher climb continues level
-    // by level.
+    // while its parent's key is greater.  On the benchmark mesh 69 % of the
+    // window pushes do not move and 11.6 % climb past four levels.  Four
+    // ancestors are loaded per round trip (they are what the level-by-level
+    // loop would read: a move only writes below the next ancestor); the number
+    // of moves over them is counted with the same stop rule and the moves are
+    // written predicated, so no data-dependent branch splits the lanes; with
+    // SVG_UP_BATCHES a longer climb takes the next four the same way, else it
+    // continues level by level.
     template <class T>
     __device__ __forceinline__ int sift_up(T* H, int cur, const T& x) {
         if constexpr (kCoop) {
