@@ -598,7 +598,8 @@ struct Layout {
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
-// heap entries per lane: the sift-down reads up to index cap + 15
+// heap entries per lane: the three-level sift-down reads up to index cap + 7
+// (the stride leaves 16 entries past the capacity)
 int heap_stride(int cap) { return (cap + 16 + 3) / 4 * 4; }
 
 // k_trace's grid: one thread per edge, at most 4,096 blocks of 256 (grid-stride)

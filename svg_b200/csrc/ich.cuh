@@ -800,12 +800,12 @@ struct LaneT {
 
     // The reference's sift-down (PriorityQueue.cuh:76-105): the children of
     // `cur` are compared with each other (ties go right) and the smaller moves
-    // up while it is smaller than the last element.  The keys of the children
-    // and grandchildren of `cur` are loaded together, so two levels cost one
-    // dependent round trip (reads past the heap's end stay inside the lane's
-    // array, stride >= cap + 16, and are never used); the moved entries are read
-    // again from the sectors just fetched and written with predicated stores,
-    // one exit test per two levels.
+    // up while it is smaller than the last element.  The keys of three levels
+    // below `cur` (SVG_SIFT3; two without it) are loaded together, so those
+    // levels cost one dependent round trip (reads past the heap's end stay
+    // inside the lane's array, stride >= cap + 8, and are never used); the
+    // moved entries are read again from the sectors just fetched and written
+    // with predicated stores, one exit test per round trip.
     template <class T>
     __device__ __forceinline__ int sift_down2(T* H, int n, const T& last) {
         if constexpr (kCoop) return coop_sift_down(H, n, last);
@@ -816,7 +816,7 @@ struct LaneT {
 #if SVG_SIFT3
             // keys of three levels below cur (2 + 4 + 8) in one round trip
             // (reads past the heap's end stay inside the lane's array,
-            // stride >= cap + 16, and are never used); the moved entries are
+            // stride >= cap + 8, and are never used); the moved entries are
             // read again from the sectors just fetched
             const double a = H[l].key, b = H[l + 1].key;
             const int g = cur << 2, h8 = cur << 3;
